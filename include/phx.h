@@ -1,0 +1,339 @@
+/*
+ * phx.h — C ABI of the B200-native SPPM renderer core (libphx.so).
+ *
+ * The reference (alfazet/phosphor) has no plugin or FFI: its hot path sits behind the private
+ * methods Renderer::trace_rays / emit_photons / hash_and_sort_photons / gather_flux
+ * (include/host/renderer.hpp:63-69), fed by RenderingBuffers::set_*_args
+ * (src/buffers/rendering.cpp:32-77) and the scene upload in Renderer::set_scene
+ * (src/renderer/renderer.cpp:22-57).  Each entry point below names the reference interface it
+ * replaces.  Only plain C types cross this boundary: POD structs byte-compatible with the
+ * reference's shared host/device structs (include/common/ headers, 16-byte aligned like GPU_ALIGN at
+ * include/common/constants.h:4), host pointers and sizes.  No device pointer, C++ exception or
+ * trap ever crosses it; every call returns an int status and phx_last_error() explains failures.
+ *
+ * Threading: one context owns one CUDA stream and all of its device memory.  A context is not
+ * safe to use from two threads at once; distinct contexts are independent.
+ */
+#ifndef PHX_H
+#define PHX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__) || defined(__CUDACC__)
+#define PHX_ALIGN16 __attribute__((aligned(16)))
+#define PHX_API __attribute__((visibility("default")))
+#else
+#define PHX_ALIGN16
+#define PHX_API
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------ */
+enum {
+    PHX_OK = 0,
+    PHX_E_INVALID = 1,     /* bad argument, size or handle */
+    PHX_E_OOM = 2,         /* device or host allocation failed */
+    PHX_E_CUDA = 3,        /* a CUDA runtime call failed (message in phx_last_error) */
+    PHX_E_TIMEOUT = 4,     /* a bounded device-side wait gave up (decoupled look-back) */
+    PHX_E_NO_PHOTONS = 5,  /* no photon was stored this round (renderer.cpp:117-118 traps here) */
+    PHX_E_STATE = 6,       /* call out of order (e.g. gather before trace) */
+    PHX_E_OVERFLOW = 7,    /* a fixed-capacity device structure overflowed (traversal stack) */
+    PHX_E_UNSUPPORTED = 8  /* feature not available in this build / on this device */
+};
+
+/* ---- POD layouts shared with the reference (byte-compatible) ----------------------------- */
+typedef struct PHX_ALIGN16 phx_f4 { float x, y, z, w; } phx_f4;
+typedef struct phx_f2 { float x, y; } __attribute__((aligned(8))) phx_f2;
+
+/* include/common/triangle.h:30-44 — 176 bytes */
+typedef struct PHX_ALIGN16 phx_triangle {
+    phx_f4 v0, v1, v2;
+    phx_f4 n0, n1, n2;
+    phx_f4 t0, t1, t2;
+    phx_f2 uv0, uv1, uv2;
+    uint32_t mat_index;
+    uint8_t _padding[4];
+} phx_triangle;
+
+/* include/common/material.h:7-27 */
+typedef struct PHX_ALIGN16 phx_uv_transform {
+    phx_f2 uv_offset;
+    phx_f2 uv_scale;
+    float uv_rotation;
+    uint8_t _padding[12];
+} phx_uv_transform;
+
+typedef struct PHX_ALIGN16 phx_uv_transform_block {
+    phx_uv_transform diff, emis, norm, occlusion, metal_rough, transmission;
+} phx_uv_transform_block;
+
+#define PHX_NO_TEXTURE 0xFFFFFFFFu
+
+/* include/common/material.h:36-59 — 96 bytes */
+typedef struct PHX_ALIGN16 phx_material {
+    phx_f4 base_color;
+    phx_f4 emissive;
+    phx_f4 att_color;
+    float metallic, roughness, transmission, ior, att_dist, thickness;
+    uint32_t diff_index, emis_index, norm_index, occlusion_index, metal_rough_index, transmission_index;
+} phx_material;
+
+/* include/common/light.h:9-31 — 128 bytes */
+#define PHX_LIGHT_POINT 0
+#define PHX_LIGHT_SPOT 1
+#define PHX_LIGHT_DIRECTIONAL 2
+#define PHX_LIGHT_TEXTURED 3
+typedef struct PHX_ALIGN16 phx_light {
+    phx_f4 position, power, direction, tangent, bitangent, origin;
+    phx_f4 aux; /* spot: x inner, y outer angle; textured: x tex (u32 bits), y tri_start, z tri_count, w area */
+    uint8_t kind;
+    uint8_t _padding[15];
+} phx_light;
+
+/* include/common/texture_meta.h:7-15 */
+typedef struct PHX_ALIGN16 phx_texture_meta {
+    uint32_t atlas_offset, width, height, channels;
+} phx_texture_meta;
+
+/* include/common/camera.h:7-22 — 112 bytes */
+typedef struct PHX_ALIGN16 phx_camera_params {
+    phx_f4 position, lower_left_corner, horizontal, vertical, defocus_disk_u, defocus_disk_v;
+    float defocus_angle;
+    float focus_distance;
+    uint8_t _padding[8];
+} phx_camera_params;
+
+/* include/common/bvh_node.h:6-8 — min.w = triangle index bits (-1 = inner), max.w = skip index */
+typedef struct PHX_ALIGN16 phx_bvh_node {
+    phx_f4 min;
+    phx_f4 max;
+} phx_bvh_node;
+
+/* include/common/photon_hash.h:11-19 — 48 bytes */
+typedef struct PHX_ALIGN16 phx_photon_hash_data {
+    phx_f4 origin;
+    phx_f4 cell_sizes;
+    uint32_t grid_res;
+    uint8_t _padding[12];
+} phx_photon_hash_data;
+
+/* Scene handed to phx_create: the SceneData arrays (include/host/scene_data.hpp:21-42) with the
+ * camera already resolved to CameraParams (Camera::to_params, src/renderer/camera.cpp:44-56).
+ * All arrays are copied at create time; the caller keeps ownership. */
+typedef struct phx_scene {
+    const phx_triangle *triangles;
+    uint32_t n_triangles;
+    const phx_triangle *emissive_triangles;
+    uint32_t n_emissive_triangles;
+    const phx_material *materials;
+    const phx_uv_transform_block *uv_transforms; /* one block per material */
+    uint32_t n_materials;
+    const phx_light *lights;
+    uint32_t n_lights;
+    const float *lum_pref_sum; /* n_lights entries (scene_data.cpp:14-23) */
+    const phx_texture_meta *tex_meta;
+    uint32_t n_textures;
+    const uint8_t *tex_atlas;
+    uint64_t tex_atlas_bytes;
+    const float *envmap; /* RGB f32, width*height*3, NULL for none */
+    uint32_t envmap_width, envmap_height; /* `camera` lands on offset 128: no implicit padding */
+    phx_camera_params camera;
+} phx_scene;
+
+/* The per-render knobs of ArgsList (include/host/cmd_args.hpp:36-65) that the pipeline uses. */
+typedef struct phx_params {
+    uint32_t width, height;        /* -w -h */
+    uint32_t photons_per_round;    /* -p */
+    uint32_t max_photon_bounces;   /* --max-bounces (1..32) */
+    uint32_t grid_res;             /* --grid-res (1..255) */
+    float sppm_alpha;              /* --sppm-alpha */
+    uint32_t direct_samples;       /* --direct-samples (1..128) */
+    uint32_t seed;                 /* --seed */
+    uint32_t flags;                /* PHX_F_* */
+    uint32_t reserved[7];
+} phx_params;
+
+/* flags */
+#define PHX_F_DEFAULT 0u
+#define PHX_F_SIMPLE_TRAVERSAL 1u /* one-thread-per-ray kernels instead of the persistent ones */
+
+/* Counters and sizes of a context. */
+typedef struct phx_info {
+    uint32_t n_pixels;
+    uint32_t width, height;
+    uint32_t photons_per_round;
+    uint32_t photon_buf_size;     /* photons_per_round * max_photon_bounces (renderer.cpp:40) */
+    uint32_t bucket_count;        /* grid_res^3 + 1 (renderer.cpp:38) */
+    uint32_t n_photons;           /* photons stored by the last emit (device value, synced) */
+    uint32_t n_bvh_nodes;
+    uint32_t bvh_depth;
+    uint32_t rounds_done;
+    uint64_t total_photons_emitted;
+    uint32_t stack_overflows;     /* traversal stack overflows seen (0 expected) */
+    uint32_t error_flags;         /* device error bits (look-back timeouts etc.) */
+    uint32_t _pad0[2];            /* keeps `hash` 16-byte aligned without implicit padding */
+    phx_photon_hash_data hash;
+    uint32_t kernels_per_round;   /* CUDA kernels one round launches (all scenes of an engine) */
+    uint32_t sort_passes;         /* counting-sort digit passes per round */
+    uint32_t reserved[6];
+} phx_info;
+
+/* Buffers readable / writable through phx_read_buffer / phx_write_buffer, always in the
+ * reference's layout (element sizes in parentheses). */
+enum {
+    PHX_BUF_HP_POS = 0,        /* float4 per pixel */
+    PHX_BUF_HP_NORMAL = 1,     /* float4 */
+    PHX_BUF_HP_THROUGHPUT = 2, /* float4 */
+    PHX_BUF_HP_BASE_COLOR = 3, /* float4 */
+    PHX_BUF_HP_DIRECT = 4,     /* float4 */
+    PHX_BUF_HP_EMISSION = 5,   /* float4 (.w = 1 when the pixel has a diffuse hit point) */
+    PHX_BUF_FLUX = 6,          /* float4 (.w = search radius squared) */
+    PHX_BUF_PHOTON_WEIGHT = 7, /* f32 */
+    PHX_BUF_RADIANCE = 8,      /* float4 */
+    PHX_BUF_PHOTON_POS = 9,    /* float4 per stored photon, canonical emission order */
+    PHX_BUF_PHOTON_POWER = 10, /* u32 RGBE */
+    PHX_BUF_PHOTON_DIR = 11,   /* u32 octahedral */
+    PHX_BUF_PHOTON_HASH = 12,  /* u32 cell key per stored photon (canonical order) */
+    PHX_BUF_CELL_COUNT = 13,   /* u32 per cell (bucket_count) */
+    PHX_BUF_CELL_START = 14,   /* u32 per cell */
+    PHX_BUF_CELL_END = 15,     /* u32 per cell */
+    PHX_BUF_SORTED_POS = 16,   /* float4 per stored photon, cell order */
+    PHX_BUF_SORTED_POWER = 17, /* u32 */
+    PHX_BUF_SORTED_DIR = 18,   /* u32 */
+    PHX_BUF_EMIT_COUNT = 19,   /* u32 photons stored by each emitted photon path */
+    PHX_BUF_BVH_NODES = 20,    /* phx_bvh_node, reference layout */
+    PHX_BUF_SORT_PERM = 21,    /* u32 canonical index of each cell-ordered photon */
+    PHX_BUF__COUNT = 22
+};
+
+/* ---- context lifecycle -------------------------------------------------------------------- */
+
+/* Replaces Renderer::Renderer + Renderer::set_scene (renderer.cpp:9-57): builds the BVH on the
+ * host with the reference's median split (bvh.cpp:18-84), uploads the scene, sizes every buffer
+ * like set_scene does, seeds the round RNG with pcg_seed(params->seed) (renderer.cpp:54).
+ * device = CUDA ordinal. */
+PHX_API int phx_create(const phx_scene *scene, const phx_params *params, int device, void **out_ctx);
+PHX_API int phx_destroy(void *ctx);
+PHX_API int phx_get_info(void *ctx, phx_info *out);
+
+/* ---- per-pass stages (the plain form: one launch sequence per pass, like the reference) ---- */
+
+/* Renderer::trace_rays (renderer.cpp:90-95) -> kernels/trace_rays.cl:14-169. */
+PHX_API int phx_trace_rays(void *ctx, uint32_t seed);
+/* Renderer::emit_photons (renderer.cpp:97-121) -> kernels/emit_photons.cl:12-114; photons are
+ * stored in canonical order (path index, then bounce).  Reads the stored count back to the host
+ * like renderer.cpp:114 and returns PHX_E_NO_PHOTONS when it is zero. */
+PHX_API int phx_emit_photons(void *ctx, uint32_t seed);
+/* Renderer::hash_and_sort_photons (renderer.cpp:123-153): hash_photons.cl, the scan_*.cl trio and
+ * scatter_photons.cl, as hash + decoupled-look-back scan + stable counting sort. */
+PHX_API int phx_hash_sort(void *ctx);
+/* Renderer::gather_flux (renderer.cpp:155-161) -> kernels/gather_flux.cl:5-78. */
+PHX_API int phx_gather(void *ctx, float sppm_alpha);
+/* One round of Renderer::run's loop body (renderer.cpp:64-78) in the plain form: draws the round
+ * seed from the context RNG, then the four stages above with the reference's two host syncs. */
+PHX_API int phx_round(void *ctx);
+/* `rounds` rounds with every stage of a round replayed from one captured CUDA graph and no host
+ * sync inside; numerically identical to calling phx_round `rounds` times. */
+PHX_API int phx_iterate(void *ctx, uint32_t rounds);
+/* One round replayed from a captured graph with the round seed given by the host, as in
+ * renderer.cpp:65 (the seed is copied from pinned memory on the context stream).  Asynchronous:
+ * returns after enqueueing; phx_sync or any read waits for it. */
+PHX_API int phx_round_seeded(void *ctx, uint32_t seed);
+PHX_API int phx_sync(void *ctx);
+
+/* Device state access in the reference layouts (for parity checks and snapshots). */
+PHX_API int phx_read_buffer(void *ctx, int which, void *dst, uint64_t offset_bytes, uint64_t bytes);
+PHX_API int phx_write_buffer(void *ctx, int which, const void *src, uint64_t offset_bytes, uint64_t bytes);
+/* Sets the stored-photon count (after writing PHOTON_POS/POWER/DIR for a stage-isolated run). */
+PHX_API int phx_set_n_photons(void *ctx, uint32_t n_photons);
+
+/* Image formation of src/renderer/output.cpp:52-83 on the device (flux / (pi r^2 N_emitted) plus
+ * radiance / rounds, exposure, optional ACES, gamma 1/2.2, clamp).  Writes width*height*3 floats
+ * in [0,1] to rgb_out (host) when rgb_out != NULL, and the u8 quantisation to ldr_out when != NULL. */
+PHX_API int phx_image(void *ctx, float exposure, int tonemap, uint64_t total_photons, uint32_t rounds,
+                      float *rgb_out, uint8_t *ldr_out);
+
+/* Host-side helpers (no GPU needed). */
+/* Bvh::Bvh (src/renderer/bvh.cpp:74-84): writes 2n-1 nodes; returns the tree depth in *depth. */
+PHX_API int phx_bvh_build(const phx_triangle *tris, uint32_t n, phx_bvh_node *out_nodes, uint32_t *depth);
+/* build_photon_hash_info (include/common/photon_hash.h:41-50) from the BVH root box. */
+PHX_API int phx_hash_info(const phx_bvh_node *root, uint32_t grid_res, phx_photon_hash_data *out);
+/* Camera::Camera + Camera::focus + Camera::to_params (src/renderer/camera.cpp:3-56). */
+PHX_API int phx_camera_make(const float position[3], const float look_at[3], const float up[3], float hfov_deg,
+                            float aspect, float defocus_angle, float focus_distance, phx_camera_params *out);
+/* SceneData::build_lum_pref_sum (src/renderer/scene_data.cpp:14-23). */
+PHX_API int phx_lum_pref_sum(const phx_light *lights, uint32_t n, float *out);
+
+/* ---- procedural scenes (the reference's .glb assets are not available) --------------------- */
+enum {
+    PHX_SCENE_CORNELL = 0,       /* empty Cornell box, 12 triangles */
+    PHX_SCENE_CAUSTIC = 1,       /* Cornell box + sine-wave water + conductor sphere */
+    PHX_SCENE_ATRIUM = 2,        /* procedural courtyard, columns, arches, boxes, sky */
+};
+typedef struct phx_scene_spec {
+    int kind;
+    uint32_t seed;
+    uint32_t width, height;      /* used for the camera aspect */
+    uint32_t detail;             /* generator-specific size knob, 0 = the configuration's size */
+    uint32_t reserved[5];
+} phx_scene_spec;
+/* Generates a scene; *out points into library-owned host memory until phx_scene_free(handle). */
+PHX_API int phx_scene_generate(const phx_scene_spec *spec, phx_scene *out, void **handle);
+PHX_API int phx_scene_free(void *handle);
+
+/* ---- batched scenes: one launch per stage for many scenes ---------------------------------- */
+/* Creates one engine over n scenes with per-scene params (uneven sizes allowed). */
+PHX_API int phx_batch_create(const phx_scene *scenes, const phx_params *params, uint32_t n, int device,
+                             void **out_batch);
+PHX_API int phx_batch_destroy(void *batch);
+/* mode 0: plain form, scenes one at a time with per-pass launches and host syncs;
+ * mode 1: all scenes per launch, each round replayed from a captured CUDA graph. */
+PHX_API int phx_batch_iterate(void *batch, uint32_t rounds, int mode);
+PHX_API int phx_batch_read_buffer(void *batch, uint32_t scene, int which, void *dst, uint64_t offset_bytes,
+                                  uint64_t bytes);
+PHX_API int phx_batch_get_info(void *batch, uint32_t scene, phx_info *out);
+PHX_API int phx_batch_image(void *batch, uint32_t scene, float exposure, int tonemap, float *rgb_out);
+
+/* ---- launch tuning -------------------------------------------------------------------------- */
+typedef struct phx_tuning {
+    uint32_t trace_block;       /* threads per block, trace kernel */
+    uint32_t emit_block;        /* threads per block, photon kernel */
+    uint32_t gather_block;      /* threads per block, gather kernel */
+    uint32_t trace_blocks_per_sm;  /* persistent grid: resident blocks per SM */
+    uint32_t emit_blocks_per_sm;
+    uint32_t persistent;        /* 1 = persistent lane-refill kernels, 0 = one thread per item */
+    uint32_t reserved[6];
+} phx_tuning;
+PHX_API int phx_get_tuning(void *ctx, phx_tuning *out);
+PHX_API int phx_set_tuning(void *ctx, const phx_tuning *in);
+
+/* ---- measurement ------------------------------------------------------------------------------ */
+/* Records CUDA events around every stage of every later round (in graph replays too) and keeps
+ * per-stage averages; enabling or disabling drops the captured graph. */
+PHX_API int phx_profile(void *ctx, int enable);
+/* Average milliseconds per round of each stage since phx_profile(ctx, 1), in the order
+ * seeds, trace, emit, emit scan + compaction, hash, cell scan, sort, records, gather (n >= 9). */
+PHX_API int phx_stage_ms(void *ctx, float *out, uint32_t n);
+/* The CUDA stream (cudaStream_t) every stage of the context or batch is enqueued on. */
+PHX_API uint64_t phx_get_stream(void *ctx);
+
+/* ---- failure detection self-test ----------------------------------------------------------------
+ * Runs the decoupled look-back scan over n elements with tile 0 withheld (the tile ticket counter
+ * starts at 1), so every other tile waits on a predecessor that never publishes.  The bounded
+ * wait must give up, set the device error flag and let the kernel finish; the call returns
+ * PHX_E_TIMEOUT with the flag in *err_flags.  No reference counterpart (the reference has no
+ * device-side waits). */
+PHX_API int phx_selftest_lookback_timeout(int device, uint32_t n, uint32_t *err_flags);
+
+PHX_API const char *phx_last_error(void);
+PHX_API const char *phx_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHX_H */

@@ -1,0 +1,358 @@
+// capi.cu — the extern "C" boundary of libphx.so (declared in include/phx.h).  Every entry point
+// validates its handle and arguments, catches every C++ exception and reports failures as status
+// codes with a message in phx_last_error(); nothing traps or throws across the boundary.
+#include "engine.hpp"
+
+#include <cstring>
+#include <new>
+
+using namespace phx;
+
+// byte layouts shared with the reference (include/common/*.h) and with the ctypes mirror
+static_assert(sizeof(phx_triangle) == 176, "Triangle layout");
+static_assert(sizeof(phx_material) == 96, "Material layout");
+static_assert(sizeof(phx_uv_transform_block) == 192, "UvTransformBlock layout");
+static_assert(sizeof(phx_light) == 128, "Light layout");
+static_assert(sizeof(phx_camera_params) == 112, "CameraParams layout");
+static_assert(sizeof(phx_bvh_node) == 32, "BvhNode layout");
+static_assert(sizeof(phx_photon_hash_data) == 48, "PhotonHashData layout");
+static_assert(sizeof(phx_texture_meta) == 16, "TextureMeta layout");
+static_assert(offsetof(phx_scene, camera) == 128 && sizeof(phx_scene) == 240, "phx_scene layout");
+static_assert(offsetof(phx_info, hash) == 64 && sizeof(phx_info) == 144, "phx_info layout");
+static_assert(sizeof(phx_params) == 64 && sizeof(phx_tuning) == 48 && sizeof(phx_scene_spec) == 40, "param layout");
+
+namespace {
+
+template <class F> int guard(F &&f) {
+    try {
+        return f();
+    } catch (const std::bad_alloc &) {
+        return fail(PHX_E_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(PHX_E_INVALID, e.what());
+    } catch (...) {
+        return fail(PHX_E_INVALID, "unknown C++ exception");
+    }
+}
+
+Engine *eng(void *h) { return reinterpret_cast<Engine *>(h); }
+
+struct SceneHandle {
+    SceneStore store;
+};
+
+} // namespace
+
+extern "C" {
+
+PHX_API const char *phx_last_error(void) { return g_last_error.c_str(); }
+PHX_API const char *phx_version(void) { return "phx 0.1 (sm_100a)"; }
+
+PHX_API int phx_create(const phx_scene *scene, const phx_params *params, int device, void **out_ctx) {
+    return guard([&]() -> int {
+        if (!out_ctx || !scene || !params)
+            return fail(PHX_E_INVALID, "null argument");
+        *out_ctx = nullptr;
+        auto *e = new Engine();
+        int r = e->create(scene, params, 1, device);
+        if (r) {
+            std::string msg = g_last_error;
+            delete e;
+            return fail(r, msg);
+        }
+        *out_ctx = e;
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_destroy(void *ctx) {
+    return guard([&]() -> int {
+        if (!ctx)
+            return fail(PHX_E_INVALID, "null context");
+        delete eng(ctx);
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_get_info(void *ctx, phx_info *out) {
+    return guard([&]() -> int { return ctx ? eng(ctx)->info(0, out) : fail(PHX_E_INVALID, "null context"); });
+}
+
+PHX_API int phx_trace_rays(void *ctx, uint32_t seed) {
+    return guard([&]() -> int {
+        if (!ctx)
+            return fail(PHX_E_INVALID, "null context");
+        Engine *e = eng(ctx);
+        int r = e->set_seed(seed);
+        if (r)
+            return r;
+        e->enq_trace();
+        cudaError_t c = cudaGetLastError();
+        return c == cudaSuccess ? PHX_OK : fail(PHX_E_CUDA, cudaGetErrorString(c));
+    });
+}
+
+PHX_API int phx_emit_photons(void *ctx, uint32_t seed) {
+    return guard([&]() -> int {
+        if (!ctx)
+            return fail(PHX_E_INVALID, "null context");
+        Engine *e = eng(ctx);
+        int r = e->set_seed(seed);
+        if (r)
+            return r;
+        e->enq_emit();
+        uint32_t n = 0;
+        if ((r = e->read_total(&n))) // renderer.cpp:113-115
+            return r;
+        e->sc[0].n_photons_last = n;
+        if (n == 0)
+            return fail(PHX_E_NO_PHOTONS, "no photon hit (renderer.cpp:117-118)");
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_hash_sort(void *ctx) {
+    return guard([&]() -> int {
+        if (!ctx)
+            return fail(PHX_E_INVALID, "null context");
+        Engine *e = eng(ctx);
+        if (!(e->stage_state & 2))
+            return fail(PHX_E_STATE, "hash_sort before emit_photons");
+        e->enq_hash_sort();
+        return e->sync_and_check();
+    });
+}
+
+PHX_API int phx_gather(void *ctx, float alpha) {
+    return guard([&]() -> int {
+        if (!ctx)
+            return fail(PHX_E_INVALID, "null context");
+        Engine *e = eng(ctx);
+        if ((e->stage_state & 5) != 5)
+            return fail(PHX_E_STATE, "gather before trace_rays and hash_sort");
+        if (!(alpha >= 0.0f))
+            return fail(PHX_E_INVALID, "sppm_alpha must be non-negative");
+        if (alpha != e->sc[0].desc.alpha) {
+            int r = e->set_alpha(alpha);
+            if (r)
+                return r;
+        }
+        e->enq_gather();
+        return e->sync_and_check(); // renderer.cpp:160
+    });
+}
+
+PHX_API int phx_round(void *ctx) {
+    return guard([&]() -> int { return ctx ? eng(ctx)->plain_round() : fail(PHX_E_INVALID, "null context"); });
+}
+
+PHX_API int phx_iterate(void *ctx, uint32_t rounds) {
+    return guard([&]() -> int { return ctx ? eng(ctx)->graph_rounds(rounds) : fail(PHX_E_INVALID, "null context"); });
+}
+
+PHX_API int phx_round_seeded(void *ctx, uint32_t seed) {
+    return guard([&]() -> int { return ctx ? eng(ctx)->seeded_round(seed) : fail(PHX_E_INVALID, "null context"); });
+}
+
+PHX_API int phx_sync(void *ctx) {
+    return guard([&]() -> int { return ctx ? eng(ctx)->sync_and_check() : fail(PHX_E_INVALID, "null context"); });
+}
+
+PHX_API int phx_read_buffer(void *ctx, int which, void *dst, uint64_t off, uint64_t bytes) {
+    return guard([&]() -> int { return ctx ? eng(ctx)->read_buffer(0, which, dst, off, bytes) : fail(PHX_E_INVALID, "null context"); });
+}
+
+PHX_API int phx_write_buffer(void *ctx, int which, const void *src, uint64_t off, uint64_t bytes) {
+    return guard([&]() -> int { return ctx ? eng(ctx)->write_buffer(0, which, src, off, bytes) : fail(PHX_E_INVALID, "null context"); });
+}
+
+PHX_API int phx_set_n_photons(void *ctx, uint32_t n) {
+    return guard([&]() -> int { return ctx ? eng(ctx)->set_n_photons(n) : fail(PHX_E_INVALID, "null context"); });
+}
+
+PHX_API int phx_image(void *ctx, float exposure, int tonemap, uint64_t total_photons, uint32_t rounds, float *rgb,
+                      uint8_t *ldr) {
+    return guard([&]() -> int {
+        return ctx ? eng(ctx)->image(0, exposure, tonemap, total_photons, rounds, rgb, ldr)
+                   : fail(PHX_E_INVALID, "null context");
+    });
+}
+
+PHX_API int phx_bvh_build(const phx_triangle *tris, uint32_t n, phx_bvh_node *out, uint32_t *depth) {
+    return guard([&]() -> int {
+        if (!tris || !out || n == 0)
+            return fail(PHX_E_INVALID, "bad arguments");
+        std::vector<phx_bvh_node> nodes;
+        if (!bvh_build(tris, n, nodes, depth))
+            return fail(PHX_E_INVALID, "degenerate or infinite triangle bounding box");
+        std::memcpy(out, nodes.data(), nodes.size() * sizeof(phx_bvh_node));
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_hash_info(const phx_bvh_node *root, uint32_t grid_res, phx_photon_hash_data *out) {
+    return guard([&]() -> int {
+        if (!root || !out || grid_res < 1 || grid_res > 255)
+            return fail(PHX_E_INVALID, "bad arguments");
+        *out = hash_info(*root, grid_res);
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_camera_make(const float position[3], const float look_at[3], const float up[3], float hfov_deg,
+                            float aspect, float defocus_angle, float focus_distance, phx_camera_params *out) {
+    return guard([&]() -> int {
+        if (!position || !look_at || !up || !out || !(aspect > 0.0f))
+            return fail(PHX_E_INVALID, "bad arguments");
+        return camera_make(position, look_at, up, hfov_deg, aspect, defocus_angle, focus_distance, out);
+    });
+}
+
+PHX_API int phx_lum_pref_sum(const phx_light *lights, uint32_t n, float *out) {
+    return guard([&]() -> int {
+        if ((!lights || !out) && n)
+            return fail(PHX_E_INVALID, "bad arguments");
+        lum_pref_sum(lights, n, out);
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_scene_generate(const phx_scene_spec *spec, phx_scene *out, void **handle) {
+    return guard([&]() -> int {
+        if (!spec || !out || !handle)
+            return fail(PHX_E_INVALID, "null argument");
+        auto *h = new SceneHandle();
+        std::string err;
+        int r = scene_generate(*spec, h->store, err);
+        if (r) {
+            delete h;
+            return fail(r, err);
+        }
+        h->store.view(out);
+        *handle = h;
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_scene_free(void *handle) {
+    return guard([&]() -> int {
+        if (!handle)
+            return fail(PHX_E_INVALID, "null handle");
+        delete reinterpret_cast<SceneHandle *>(handle);
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_batch_create(const phx_scene *scenes, const phx_params *params, uint32_t n, int device,
+                             void **out_batch) {
+    return guard([&]() -> int {
+        if (!out_batch || !scenes || !params || n == 0)
+            return fail(PHX_E_INVALID, "bad arguments");
+        *out_batch = nullptr;
+        auto *e = new Engine();
+        int r = e->create(scenes, params, n, device);
+        if (r) {
+            std::string msg = g_last_error;
+            delete e;
+            return fail(r, msg);
+        }
+        *out_batch = e;
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_batch_destroy(void *b) { return phx_destroy(b); }
+
+PHX_API int phx_batch_iterate(void *b, uint32_t rounds, int mode) {
+    return guard([&]() -> int {
+        if (!b)
+            return fail(PHX_E_INVALID, "null batch");
+        Engine *e = eng(b);
+        if (mode == 1)
+            return e->graph_rounds(rounds);
+        if (mode != 0)
+            return fail(PHX_E_INVALID, "mode must be 0 or 1");
+        for (uint32_t i = 0; i < rounds; i++) {
+            int r = e->plain_round();
+            if (r)
+                return r;
+        }
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_batch_read_buffer(void *b, uint32_t scene, int which, void *dst, uint64_t off, uint64_t bytes) {
+    return guard([&]() -> int { return b ? eng(b)->read_buffer(scene, which, dst, off, bytes) : fail(PHX_E_INVALID, "null batch"); });
+}
+
+PHX_API int phx_batch_get_info(void *b, uint32_t scene, phx_info *out) {
+    return guard([&]() -> int { return b ? eng(b)->info(scene, out) : fail(PHX_E_INVALID, "null batch"); });
+}
+
+PHX_API int phx_batch_image(void *b, uint32_t scene, float exposure, int tonemap, float *rgb) {
+    return guard([&]() -> int { return b ? eng(b)->image(scene, exposure, tonemap, 0, 0, rgb, nullptr) : fail(PHX_E_INVALID, "null batch"); });
+}
+
+PHX_API int phx_get_tuning(void *ctx, phx_tuning *out) {
+    return guard([&]() -> int {
+        if (!ctx || !out)
+            return fail(PHX_E_INVALID, "null argument");
+        *out = eng(ctx)->tune;
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_set_tuning(void *ctx, const phx_tuning *in) {
+    return guard([&]() -> int {
+        if (!ctx || !in)
+            return fail(PHX_E_INVALID, "null argument");
+        const uint32_t blocks[3] = {in->trace_block, in->emit_block, in->gather_block};
+        for (uint32_t b : blocks)
+            if (b != 0 && (b % 32 != 0 || b > 1024))
+                return fail(PHX_E_INVALID, "block sizes must be multiples of 32 up to 1024");
+        if (in->trace_blocks_per_sm > 64 || in->emit_blocks_per_sm > 64)
+            return fail(PHX_E_INVALID, "blocks_per_sm out of range");
+        Engine *e = eng(ctx);
+        e->tune = *in;
+        e->invalidate_graph(); // the next replay is captured with the new launch shape
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_profile(void *ctx, int enable) {
+    return guard([&]() -> int {
+        if (!ctx)
+            return fail(PHX_E_INVALID, "null context");
+        eng(ctx)->set_profiling(enable != 0);
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_stage_ms(void *ctx, float *out, uint32_t n) {
+    return guard([&]() -> int {
+        if (!ctx || !out || n < (uint32_t)ST__N)
+            return fail(PHX_E_INVALID, "need room for every stage");
+        eng(ctx)->stage_ms(out);
+        return PHX_OK;
+    });
+}
+
+PHX_API uint64_t phx_get_stream(void *ctx) { return ctx ? (uint64_t)(uintptr_t)eng(ctx)->st : 0; }
+
+PHX_API int phx_selftest_lookback_timeout(int device, uint32_t n, uint32_t *err_flags) {
+    return guard([&]() -> int {
+        if (!err_flags || n == 0 || n > (1u << 26))
+            return fail(PHX_E_INVALID, "bad arguments");
+        *err_flags = 0;
+        int rc = selftest_lookback_timeout(device, n, err_flags);
+        if (rc == 2)
+            return fail(PHX_E_OOM, "self-test allocation failed");
+        if (rc == 3)
+            return fail(PHX_E_CUDA, "self-test kernel failed");
+        if (*err_flags & ERR_LOOKBACK_TIMEOUT)
+            return fail(PHX_E_TIMEOUT, "look-back wait gave up as intended (tile 0 withheld)");
+        return PHX_OK;
+    });
+}
+
+} // extern "C"

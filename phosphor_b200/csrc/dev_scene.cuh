@@ -1,0 +1,225 @@
+// dev_scene.cuh — per-scene device descriptor and closest-hit BVH traversal.
+//
+// BVH layout.  The host builds the reference's tree (median split, one triangle per leaf,
+// depth-first flattening: src/renderer/bvh.cpp:18-84) and re-packs it for the device:
+//  * inner nodes in pre-order, each a 64-byte "child pair" of four float4: both children's
+//    boxes side by side so one node fetch (four coalesced 16-byte loads) tests both children;
+//  * child references: >= 0 inner node index, < 0 ~leaf rank;
+//  * triangles in leaf (pre-)order as 48-byte records {v0 | mat bits, v1-v0, v2-v0}, so the leaf
+//    rank is also the triangle's device index and all per-triangle shading data is stored in
+//    that order.
+// Traversal visits the nearer child first and culls popped entries whose entry distance exceeds
+// the current closest hit.  The reference's depth-first left-first order (hit.h:135-172) keeps
+// the LAST tested triangle among hits at exactly equal t (`t > t_max` rejects, equality passes,
+// hit.h:68); with left-first pre-order that is the equal-t hit with the largest leaf rank, so an
+// equal-t candidate replaces the current hit only when its rank is larger.  Boxes are expanded by
+// 1e-3 (bounding_box.h:30-37), so no box that holds the closest hit is ever culled by either
+// order, and the result is the reference's hit for every ray.  The reference drops children when
+// its 24-entry stack is full (hit.h:163-164), which only happens for trees deeper than 22 levels;
+// the host reports the depth and this traversal counts (instead of silently dropping) overflows
+// of its own 64-entry stack.
+#pragma once
+
+#include "dev_common.cuh"
+
+namespace phx {
+
+struct __align__(16) SceneDesc {
+    // geometry, device pointers
+    const float4 *cnodes;   // 4 float4 per inner node
+    const float4 *trirec;   // 3 float4 per triangle (leaf order)
+    const float4 *tri_nrm;  // n0,n1,n2 per triangle (leaf order)
+    const float4 *tri_tan;  // t0,t1,t2
+    const float4 *tri_uv;   // (uv0.xy, uv1.xy), (uv2.xy, 0, 0)
+    const float4 *etri_v;   // emissive triangles v0,v1,v2
+    const float4 *etri_n;   // n0,n1,n2
+    const float4 *etri_uv;  // 2 float4 per emissive triangle
+    const u32 *etri_mat;
+    const phx_material *materials;
+    const phx_uv_transform_block *uvt;
+    const phx_texture_meta *tex_meta;
+    const u8 *tex_atlas;
+    const phx_light *lights;
+    const float *lum_pref_sum;
+    const float *envmap;
+    i32 root;       // root reference (>= 0 inner, < 0 ~leaf)
+    u32 n_tris;
+    u32 n_lights;
+    float total_lum;
+    float4 scene_center;
+    float scene_radius;
+    u32 env_w, env_h, has_env;
+    phx_camera_params camera;
+    // image and photon budget
+    u32 width, height, n_pixels;
+    u32 n_emit;           // photons emitted per round
+    u32 max_bounces;
+    u32 direct_samples;
+    float alpha;
+    u32 n_cells;          // grid_res^3 + 1
+    GridDev grid;
+    // bases in the engine's concatenated arrays
+    u32 pixel_base;       // first pixel of this scene
+    u32 emit_base;        // first photon path of this scene
+    u32 cell_base;        // first cell of this scene
+    u32 pad0;
+    u64 slot_base;        // first photon slot of this scene (slot j of path t at slot_base + j*n_emit + t)
+    u32 flags;
+    u32 any_transmissive; // 0 -> shadow rays can stop at the first hit
+    u32 pad1[2];
+};
+
+// scene of global index gid: bases[s] <= gid < bases[s+1] (n+1 prefix offsets)
+PHX_DI u32 find_scene(const u32 *bases, u32 n, u32 gid) {
+    u32 lo = 0, hi = n;
+    while (hi - lo > 1) {
+        u32 mid = (lo + hi) >> 1;
+        if (__ldg(&bases[mid]) <= gid)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// ---- closest hit ------------------------------------------------------------------------------
+struct Hit {
+    float t, u, v;
+    i32 tri; // device triangle index (leaf rank), -1 = none
+};
+
+constexpr int TRAV_STACK = 64;
+
+// Möller–Trumbore test of hit.h:45-78 with the reference's dot(float4) including w terms.
+// ow, dw: w components of the ray origin and direction (always +-0 in practice).
+PHX_DI bool tri_test(const float4 *rec, float ox, float oy, float oz, float ow, float dx, float dy, float dz, float dw,
+                     float t_min, float t_max, float *tt, float *tu, float *tv) {
+    float4 r0 = __ldg(rec + 0), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2);
+    // e1 = r1.xyz, e2 = r2.xyz (precomputed v1-v0, v2-v0 with the same float subtraction)
+    float hx = dy * r2.z - dz * r2.y;
+    float hy = dz * r2.x - dx * r2.z;
+    float hz = dx * r2.y - dy * r2.x;
+    float a = ((r1.x * hx + r1.y * hy) + r1.z * hz) + 0.0f * 0.0f;
+    if (fabsf(a) < EPS)
+        return false;
+    float f = 1.0f / a;
+    float sx = ox - r0.x, sy = oy - r0.y, sz = oz - r0.z, sw = ow - 0.0f;
+    float u = f * (((sx * hx + sy * hy) + sz * hz) + sw * 0.0f);
+    if (u < 0.0f || u > 1.0f)
+        return false;
+    float qx = sy * r1.z - sz * r1.y;
+    float qy = sz * r1.x - sx * r1.z;
+    float qz = sx * r1.y - sy * r1.x;
+    float v = f * (((dx * qx + dy * qy) + dz * qz) + dw * 0.0f);
+    if (v < 0.0f || u + v > 1.0f)
+        return false;
+    float t = f * (((r2.x * qx + r2.y * qy) + r2.z * qz) + 0.0f * 0.0f);
+    if (t < t_min || t > t_max)
+        return false;
+    *tt = t;
+    *tu = u;
+    *tv = v;
+    return true;
+}
+
+PHX_DI void box2(const float4 &a, const float4 &b, const float4 &c, float ix, float iy, float iz, float ox, float oy,
+                 float oz, float t_min, float t_max, float *tl, float *tr, bool *hl, bool *hr) {
+    // left child: a = (minx, maxx, miny, maxy), c.xy = (minz, maxz); right: b, c.zw
+    float lx0 = (a.x - ox) * ix, lx1 = (a.y - ox) * ix;
+    float ly0 = (a.z - oy) * iy, ly1 = (a.w - oy) * iy;
+    float lz0 = (c.x - oz) * iz, lz1 = (c.y - oz) * iz;
+    float rx0 = (b.x - ox) * ix, rx1 = (b.y - ox) * ix;
+    float ry0 = (b.z - oy) * iy, ry1 = (b.w - oy) * iy;
+    float rz0 = (c.z - oz) * iz, rz1 = (c.w - oz) * iz;
+    float lnear = fmaxf(fmaxf(fminf(lx0, lx1), fminf(ly0, ly1)), fmaxf(fminf(lz0, lz1), t_min));
+    float lfar = fminf(fminf(fmaxf(lx0, lx1), fmaxf(ly0, ly1)), fminf(fmaxf(lz0, lz1), t_max));
+    float rnear = fmaxf(fmaxf(fminf(rx0, rx1), fminf(ry0, ry1)), fmaxf(fminf(rz0, rz1), t_min));
+    float rfar = fminf(fminf(fmaxf(rx0, rx1), fmaxf(ry0, ry1)), fminf(fmaxf(rz0, rz1), t_max));
+    *tl = lnear;
+    *tr = rnear;
+    *hl = lnear <= lfar;
+    *hr = rnear <= rfar;
+}
+
+// Closest hit in [t_min, t_max] (scene_intersect, hit.h:135-172).  Returns false on a miss.
+// `any` stops at the first accepted hit (only valid where the caller needs no specific hit).
+PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, float t_max, Hit *hit, u32 *overflow,
+                      bool any = false) {
+    float ix = 1.0f / d.x, iy = 1.0f / d.y, iz = 1.0f / d.z;
+    float closest = t_max;
+    i32 best = -1;
+    float bu = 0.0f, bv = 0.0f;
+    i32 stack_ref[TRAV_STACK];
+    float stack_t[TRAV_STACK];
+    int sp = 0;
+    i32 node = sc.root;
+    for (;;) {
+        while (node >= 0) {
+            const float4 *cn = sc.cnodes + 4 * (size_t)node;
+            float4 a = __ldg(cn + 0), b = __ldg(cn + 1), c = __ldg(cn + 2);
+            int4 ch = __ldg(reinterpret_cast<const int4 *>(cn + 3));
+            float tl, tr;
+            bool hl, hr;
+            box2(a, b, c, ix, iy, iz, o.x, o.y, o.z, t_min, closest, &tl, &tr, &hl, &hr);
+            if (hl && hr) {
+                i32 nearr = ch.x, farr = ch.y;
+                float tfar = tr;
+                if (tr < tl) {
+                    nearr = ch.y;
+                    farr = ch.x;
+                    tfar = tl;
+                }
+                if (sp < TRAV_STACK) {
+                    stack_ref[sp] = farr;
+                    stack_t[sp] = tfar;
+                    sp++;
+                } else {
+                    *overflow += 1;
+                }
+                node = nearr;
+            } else if (hl) {
+                node = ch.x;
+            } else if (hr) {
+                node = ch.y;
+            } else {
+                node = 0x7fffffff; // pop marker
+                break;
+            }
+        }
+        if (node != 0x7fffffff) {
+            // leaf
+            i32 rank = ~node;
+            float t, u, v;
+            if (tri_test(sc.trirec + 3 * (size_t)rank, o.x, o.y, o.z, o.w, d.x, d.y, d.z, d.w, t_min, closest, &t, &u,
+                         &v)) {
+                if (t < closest || rank > best) {
+                    closest = t;
+                    best = rank;
+                    bu = u;
+                    bv = v;
+                    if (any)
+                        break;
+                }
+            }
+        }
+        // pop the next entry that can still hold a hit
+        bool found = false;
+        while (sp > 0) {
+            sp--;
+            if (stack_t[sp] <= closest) {
+                node = stack_ref[sp];
+                found = true;
+                break;
+            }
+        }
+        if (!found)
+            break;
+    }
+    hit->t = closest;
+    hit->u = bu;
+    hit->v = bv;
+    hit->tri = best;
+    return best >= 0;
+}
+
+} // namespace phx

@@ -1,0 +1,947 @@
+// engine.cu — Engine: scene upload, device memory, stage enqueueing, the plain per-pass form
+// (Renderer::run, src/renderer/renderer.cpp:59-161, with its two host syncs per round) and the
+// graph form (one captured round replayed with no host sync).
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace phx {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CK(x)                                                                                                          \
+    do {                                                                                                               \
+        cudaError_t e_ = (x);                                                                                          \
+        if (e_ != cudaSuccess)                                                                                         \
+            return fail(PHX_E_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));                                  \
+    } while (0)
+
+void init_kernels(int device);
+
+int DevBuf::alloc(size_t b) {
+    release();
+    bytes = b;
+    if (cudaMalloc(&p, b ? b : 16) != cudaSuccess) {
+        cudaGetLastError();
+        p = nullptr;
+        return fail(PHX_E_OOM, "device allocation of " + std::to_string(b) + " bytes failed");
+    }
+    return PHX_OK;
+}
+
+void DevBuf::release() {
+    if (p)
+        cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+Engine::~Engine() {
+    if (st)
+        cudaStreamSynchronize(st);
+    invalidate_graph();
+    for (auto &e : events)
+        if (e)
+            cudaEventDestroy(e);
+    for (auto &e : seed_ev)
+        if (e)
+            cudaEventDestroy(e);
+    if (h_seed_ring)
+        cudaFreeHost(h_seed_ring);
+    for (auto &s : sc)
+        for (auto &b : s.bufs)
+            b.release();
+    DevBuf *all[] = {&d_desc, &d_pix_bases, &d_emit_bases, &d_seeds, &d_rng, &d_err, &d_ovf, &d_queue, &d_ntotal,
+                     &flux, &weight, &radiance, &slot_pos, &slot_pd, &counts, &offsets, &ph_pos, &ph_pd, &keys,
+                     &cell_count, &cell_start, &sk0, &sk1, &sv0, &sv1, &s_posdir, &s_power, &scan_scr, &radix_scr,
+                     &img_rgb, &img_ldr};
+    for (auto *b : all)
+        b->release();
+    for (auto &b : hp)
+        b.release();
+    if (h_pinned)
+        cudaFreeHost(h_pinned);
+    if (st)
+        cudaStreamDestroy(st);
+}
+
+static int upload(DevBuf &b, const void *src, size_t bytes) {
+    int r = b.alloc(bytes);
+    if (r)
+        return r;
+    if (bytes && src)
+        CK(cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice));
+    else
+        CK(cudaMemset(b.p, 0, bytes ? bytes : 16));
+    return PHX_OK;
+}
+
+static int check_params(const phx_params &p) {
+    if (p.width == 0 || p.height == 0 || (uint64_t)p.width * p.height > 0x7fffffffull)
+        return fail(PHX_E_INVALID, "image size out of range");
+    if (p.photons_per_round == 0)
+        return fail(PHX_E_INVALID, "photons_per_round must be positive");
+    if (p.max_photon_bounces < 1 || p.max_photon_bounces > 32)
+        return fail(PHX_E_INVALID, "max_photon_bounces must be in 1..32 (cmd_args.hpp:49)");
+    if (p.grid_res < 1 || p.grid_res > 255)
+        return fail(PHX_E_INVALID, "grid_res must be in 1..255 (cmd_args.hpp:51)");
+    if (p.direct_samples < 1 || p.direct_samples > 128)
+        return fail(PHX_E_INVALID, "direct_samples must be in 1..128 (cmd_args.hpp:59)");
+    if (!(p.sppm_alpha >= 0.0f))
+        return fail(PHX_E_INVALID, "sppm_alpha must be non-negative");
+    return PHX_OK;
+}
+
+int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, uint32_t *pix, uint32_t *emit,
+                         uint32_t *cell, uint64_t *slot) {
+    SceneSlot &S = sc[i];
+    S.prm = p;
+    if (!s.triangles || s.n_triangles == 0)
+        return fail(PHX_E_INVALID, "scene has no triangles");
+    if (!s.materials || s.n_materials == 0)
+        return fail(PHX_E_INVALID, "scene has no materials");
+    for (uint32_t t = 0; t < s.n_triangles; t++)
+        if (s.triangles[t].mat_index >= s.n_materials)
+            return fail(PHX_E_INVALID, "triangle material index out of range");
+    for (uint32_t l = 0; l < s.n_lights; l++)
+        if (s.lights[l].kind == PHX_LIGHT_TEXTURED) {
+            uint32_t a, b;
+            std::memcpy(&a, &s.lights[l].aux.y, 4);
+            std::memcpy(&b, &s.lights[l].aux.z, 4);
+            if ((uint64_t)a + b > s.n_emissive_triangles)
+                return fail(PHX_E_INVALID, "emissive light triangle range out of bounds");
+        }
+    if (s.n_textures && (!s.tex_meta || !s.tex_atlas))
+        return fail(PHX_E_INVALID, "textures declared without data");
+    for (uint32_t k = 0; k < s.n_textures; k++) {
+        const phx_texture_meta &m = s.tex_meta[k];
+        // texel reads stay inside the atlas (material.h:84-122 index width*height*channels bytes, and
+        // naive_sample_texture assumes 3 channels)
+        if (m.width == 0 || m.height == 0 || m.channels < 3 ||
+            (uint64_t)m.atlas_offset + (uint64_t)m.width * m.height * m.channels > s.tex_atlas_bytes)
+            return fail(PHX_E_INVALID, "texture extends past the atlas or has fewer than 3 channels");
+    }
+    if (s.envmap && (s.envmap_width == 0) != (s.envmap_height == 0))
+        return fail(PHX_E_INVALID, "envmap with a zero dimension");
+    for (uint32_t m = 0; m < s.n_materials; m++) {
+        const phx_material &mm = s.materials[m];
+        const uint32_t idx[6] = {mm.diff_index, mm.emis_index, mm.norm_index, mm.occlusion_index,
+                                 mm.metal_rough_index, mm.transmission_index};
+        for (uint32_t k : idx)
+            if (k != PHX_NO_TEXTURE && k >= s.n_textures)
+                return fail(PHX_E_INVALID, "material texture index out of range");
+    }
+    if (!bvh_build(s.triangles, s.n_triangles, S.nodes, &S.depth))
+        return fail(PHX_E_INVALID, "degenerate or infinite triangle bounding box (bounding_box.h:17-28)");
+    PackedBvh pk;
+    bvh_pack(S.nodes, s.triangles, pk);
+    const uint32_t n = s.n_triangles;
+    S.n_tris = n;
+    std::vector<float> nrm((size_t)n * 12), tan((size_t)n * 12), uv((size_t)n * 8);
+    for (uint32_t r = 0; r < n; r++) {
+        const phx_triangle &t = s.triangles[pk.leaf_tri[r]];
+        const phx_f4 *nn[3] = {&t.n0, &t.n1, &t.n2}, *tt[3] = {&t.t0, &t.t1, &t.t2};
+        for (int k = 0; k < 3; k++) {
+            std::memcpy(&nrm[(size_t)r * 12 + 4 * k], nn[k], 16);
+            std::memcpy(&tan[(size_t)r * 12 + 4 * k], tt[k], 16);
+        }
+        float u8v[8] = {t.uv0.x, t.uv0.y, t.uv1.x, t.uv1.y, t.uv2.x, t.uv2.y, 0.0f, 0.0f};
+        std::memcpy(&uv[(size_t)r * 8], u8v, 32);
+    }
+    const uint32_t ne = s.n_emissive_triangles;
+    std::vector<float> ev((size_t)std::max(ne, 1u) * 12, 0.0f), en((size_t)std::max(ne, 1u) * 12, 0.0f),
+        euv((size_t)std::max(ne, 1u) * 8, 0.0f);
+    std::vector<uint32_t> emat(std::max(ne, 1u), 0u);
+    for (uint32_t k = 0; k < ne; k++) {
+        const phx_triangle &t = s.emissive_triangles[k];
+        const phx_f4 *vv[3] = {&t.v0, &t.v1, &t.v2}, *nn[3] = {&t.n0, &t.n1, &t.n2};
+        for (int j = 0; j < 3; j++) {
+            std::memcpy(&ev[(size_t)k * 12 + 4 * j], vv[j], 16);
+            std::memcpy(&en[(size_t)k * 12 + 4 * j], nn[j], 16);
+        }
+        float u8v[8] = {t.uv0.x, t.uv0.y, t.uv1.x, t.uv1.y, t.uv2.x, t.uv2.y, 0.0f, 0.0f};
+        std::memcpy(&euv[(size_t)k * 8], u8v, 32);
+        emat[k] = t.mat_index;
+    }
+    std::vector<phx_uv_transform_block> uvt(s.n_materials);
+    if (s.uv_transforms) {
+        std::memcpy(uvt.data(), s.uv_transforms, sizeof(phx_uv_transform_block) * s.n_materials);
+    } else {
+        phx_uv_transform id{};
+        id.uv_scale = {1.0f, 1.0f};
+        for (auto &b : uvt)
+            b.diff = b.emis = b.norm = b.occlusion = b.metal_rough = b.transmission = id;
+    }
+    std::vector<float> lum(std::max(s.n_lights, 1u), 0.0f);
+    if (s.n_lights) {
+        if (s.lum_pref_sum)
+            std::memcpy(lum.data(), s.lum_pref_sum, 4 * s.n_lights);
+        else
+            lum_pref_sum(s.lights, s.n_lights, lum.data());
+    }
+    S.bufs.resize(16);
+    int r;
+    if ((r = upload(S.bufs[0], pk.cnodes.data(), pk.cnodes.size() * 4)) ||
+        (r = upload(S.bufs[1], pk.trirec.data(), pk.trirec.size() * 4)) ||
+        (r = upload(S.bufs[2], nrm.data(), nrm.size() * 4)) || (r = upload(S.bufs[3], tan.data(), tan.size() * 4)) ||
+        (r = upload(S.bufs[4], uv.data(), uv.size() * 4)) || (r = upload(S.bufs[5], ev.data(), ev.size() * 4)) ||
+        (r = upload(S.bufs[6], en.data(), en.size() * 4)) || (r = upload(S.bufs[7], euv.data(), euv.size() * 4)) ||
+        (r = upload(S.bufs[8], emat.data(), emat.size() * 4)) ||
+        (r = upload(S.bufs[9], s.materials, sizeof(phx_material) * s.n_materials)) ||
+        (r = upload(S.bufs[10], uvt.data(), sizeof(phx_uv_transform_block) * uvt.size())) ||
+        (r = upload(S.bufs[11], s.tex_meta, sizeof(phx_texture_meta) * std::max(s.n_textures, 1u))) ||
+        (r = upload(S.bufs[12], s.tex_atlas, std::max<uint64_t>(s.tex_atlas_bytes, 16))) ||
+        (r = upload(S.bufs[13], s.lights, sizeof(phx_light) * std::max(s.n_lights, 1u))) ||
+        (r = upload(S.bufs[14], lum.data(), lum.size() * 4)))
+        return r;
+    const bool has_env = s.envmap && s.envmap_width > 0 && s.envmap_height > 0;
+    if ((r = upload(S.bufs[15], has_env ? s.envmap : nullptr,
+                    has_env ? (size_t)s.envmap_width * s.envmap_height * 3 * 4 : 16)))
+        return r;
+
+    SceneDesc &d = S.desc;
+    std::memset(&d, 0, sizeof(d));
+    d.cnodes = S.bufs[0].as<float4>();
+    d.trirec = S.bufs[1].as<float4>();
+    d.tri_nrm = S.bufs[2].as<float4>();
+    d.tri_tan = S.bufs[3].as<float4>();
+    d.tri_uv = S.bufs[4].as<float4>();
+    d.etri_v = S.bufs[5].as<float4>();
+    d.etri_n = S.bufs[6].as<float4>();
+    d.etri_uv = S.bufs[7].as<float4>();
+    d.etri_mat = S.bufs[8].as<u32>();
+    d.materials = S.bufs[9].as<phx_material>();
+    d.uvt = S.bufs[10].as<phx_uv_transform_block>();
+    d.tex_meta = S.bufs[11].as<phx_texture_meta>();
+    d.tex_atlas = S.bufs[12].as<u8>();
+    d.lights = S.bufs[13].as<phx_light>();
+    d.lum_pref_sum = S.bufs[14].as<float>();
+    d.envmap = S.bufs[15].as<float>();
+    d.root = pk.root;
+    d.n_tris = n;
+    d.n_lights = s.n_lights;
+    d.total_lum = s.n_lights ? lum[s.n_lights - 1] : 0.0f; // shading.cpp:26
+    phx_f4 ctr;
+    float rad;
+    scene_sphere(S.nodes[0], &ctr, &rad);
+    d.scene_center = make_float4(ctr.x, ctr.y, ctr.z, ctr.w);
+    d.scene_radius = rad;
+    d.env_w = has_env ? s.envmap_width : 0;
+    d.env_h = has_env ? s.envmap_height : 0;
+    d.has_env = has_env ? 1u : 0u;
+    d.camera = s.camera;
+    d.width = p.width;
+    d.height = p.height;
+    d.n_pixels = p.width * p.height;
+    d.n_emit = p.photons_per_round;
+    d.max_bounces = p.max_photon_bounces;
+    d.direct_samples = p.direct_samples;
+    d.alpha = p.sppm_alpha;
+    d.n_cells = p.grid_res * p.grid_res * p.grid_res + 1; // renderer.cpp:38
+    S.hash = hash_info(S.nodes[0], p.grid_res);
+    d.grid = GridDev{S.hash.origin.x, S.hash.origin.y, S.hash.origin.z, S.hash.cell_sizes.x,
+                     S.hash.cell_sizes.y, S.hash.cell_sizes.z, p.grid_res, 0u};
+    d.pixel_base = *pix;
+    d.emit_base = *emit;
+    d.cell_base = *cell;
+    d.slot_base = *slot;
+    d.flags = p.flags;
+    d.any_transmissive = 0;
+    for (uint32_t m = 0; m < s.n_materials; m++)
+        if (s.materials[m].transmission >= 1e-5f)
+            d.any_transmissive = 1;
+    if ((uint64_t)*pix + d.n_pixels > 0x7fffffffull || (uint64_t)*emit + d.n_emit > 0x7fffffffull ||
+        (uint64_t)*cell + d.n_cells > 0x7fffffffull)
+        return fail(PHX_E_INVALID, "batch too large for 31-bit global indices");
+    *pix += d.n_pixels;
+    *emit += d.n_emit;
+    *cell += d.n_cells;
+    *slot += (uint64_t)d.n_emit * d.max_bounces;
+    return PHX_OK;
+}
+
+int Engine::create(const phx_scene *scenes, const phx_params *params, uint32_t n, int dev) {
+    if (!scenes || !params || n == 0)
+        return fail(PHX_E_INVALID, "no scenes");
+    for (uint32_t i = 0; i < n; i++) {
+        int r = check_params(params[i]);
+        if (r)
+            return r;
+    }
+    device = dev;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    init_kernels(device);
+    sc.resize(n);
+    uint32_t pix = 0, emit = 0, cell = 0;
+    uint64_t slot = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        int r = upload_scene(i, scenes[i], params[i], &pix, &emit, &cell, &slot);
+        if (r)
+            return r;
+    }
+    total_pixels = pix;
+    total_emit = emit;
+    total_cells = cell;
+    total_slots = slot;
+    max_photons = slot; // <= one stored photon per bounce (renderer.cpp:40)
+    if (max_photons > 0x7fffffffull)
+        return fail(PHX_E_INVALID, "photon buffer exceeds 2^31 entries");
+    uint32_t kmax = total_cells - 1;
+    key_bits = 1;
+    while (key_bits < 32 && (kmax >> key_bits) != 0)
+        key_bits++;
+
+    std::vector<SceneDesc> descs(n);
+    std::vector<uint32_t> pb(n + 1), eb(n + 1), rng(n);
+    for (uint32_t i = 0; i < n; i++) {
+        descs[i] = sc[i].desc;
+        pb[i] = sc[i].desc.pixel_base;
+        eb[i] = sc[i].desc.emit_base;
+        rng[i] = pcg_seed(sc[i].prm.seed).state; // renderer.cpp:54
+    }
+    pb[n] = total_pixels;
+    eb[n] = total_emit;
+    int r;
+    if ((r = upload(d_desc, descs.data(), sizeof(SceneDesc) * n)) || (r = upload(d_pix_bases, pb.data(), 4 * pb.size())) ||
+        (r = upload(d_emit_bases, eb.data(), 4 * eb.size())) || (r = upload(d_rng, rng.data(), 4 * n)) ||
+        (r = upload(d_seeds, nullptr, 4 * n)) || (r = upload(d_err, nullptr, 16)) || (r = upload(d_ovf, nullptr, 16)) ||
+        (r = upload(d_queue, nullptr, 16)) || (r = upload(d_ntotal, nullptr, 16)))
+        return r;
+    const size_t P = total_pixels, E = total_emit, C = (size_t)total_cells + 1, N = max_photons;
+    for (auto &b : hp)
+        if ((r = upload(b, nullptr, 16 * P))) // ImageBuffers::alloc zero-fills (image.cpp:11-21)
+            return r;
+    if ((r = upload(flux, nullptr, 16 * P)) || (r = upload(weight, nullptr, 4 * P)) || (r = upload(radiance, nullptr, 16 * P)) ||
+        (r = slot_pos.alloc(16 * N)) || (r = slot_pd.alloc(8 * N)) || (r = upload(counts, nullptr, 4 * (E + 1))) ||
+        (r = upload(offsets, nullptr, 4 * (E + 1))) || (r = upload(ph_pos, nullptr, 16 * N)) ||
+        (r = upload(ph_pd, nullptr, 8 * N)) || (r = upload(keys, nullptr, 4 * N)) ||
+        (r = upload(cell_count, nullptr, 4 * C)) || (r = upload(cell_start, nullptr, 4 * C)) ||
+        (r = sk0.alloc(4 * N)) || (r = sk1.alloc(4 * N)) || (r = upload(sv0, nullptr, 4 * N)) ||
+        (r = upload(sv1, nullptr, 4 * N)) || (r = upload(s_posdir, nullptr, 16 * N)) ||
+        (r = upload(s_power, nullptr, 4 * N)) ||
+        (r = scan_scr.alloc(std::max(scan_scratch_bytes(E + 1), scan_scratch_bytes(C)))) ||
+        (r = radix_scr.alloc(radix_scratch_bytes(N, key_bits))))
+        return r;
+    perm = sv0.as<u32>();
+    CK(cudaMallocHost((void **)&h_pinned, 4096));
+    tune.trace_block = 128;
+    tune.emit_block = 128;
+    tune.gather_block = 128;
+    tune.trace_blocks_per_sm = 8;
+    tune.emit_blocks_per_sm = 8;
+    tune.persistent = 0;
+    for (uint32_t i = 0; i < n; i++)
+        if (params[i].flags & PHX_F_SIMPLE_TRAVERSAL)
+            tune.persistent = 0;
+    CK(cudaDeviceSynchronize());
+    return PHX_OK;
+}
+
+LaunchCtx Engine::lc() const {
+    LaunchCtx l;
+    l.scenes = d_desc.as<SceneDesc>();
+    l.n_scenes = (u32)sc.size();
+    l.pix_bases = d_pix_bases.as<u32>();
+    l.emit_bases = d_emit_bases.as<u32>();
+    l.total_pixels = total_pixels;
+    l.total_emit = total_emit;
+    l.seeds = d_seeds.as<u32>();
+    l.err = d_err.as<u32>();
+    l.overflow = d_ovf.as<u32>();
+    return l;
+}
+
+GridBufs Engine::gb() const {
+    GridBufs g;
+    g.counts = counts.as<u32>();
+    g.offsets = offsets.as<u32>();
+    g.slot_pos = slot_pos.as<float4>();
+    g.slot_pd = slot_pd.as<uint2>();
+    g.ph_pos = ph_pos.as<float4>();
+    g.ph_pd = ph_pd.as<uint2>();
+    g.keys = keys.as<u32>();
+    g.cell_count = cell_count.as<u32>();
+    return g;
+}
+
+void Engine::ev(int stage, bool end) {
+    if (!profiling)
+        return;
+    cudaEvent_t &e = events[2 * stage + (end ? 1 : 0)];
+    if (!e)
+        cudaEventCreate(&e);
+    if (capturing)
+        cudaEventRecordWithFlags(e, st, cudaEventRecordExternal);
+    else
+        cudaEventRecord(e, st);
+}
+
+void Engine::enq_seeds() {
+    ev(ST_SEEDS, false);
+    launch_next_seeds(d_rng.as<u32>(), d_seeds.as<u32>(), (u32)sc.size(), st);
+    ev(ST_SEEDS, true);
+}
+
+void Engine::enq_trace() {
+    ev(ST_TRACE, false);
+    TraceOut o{hp[0].as<float4>(), hp[1].as<float4>(), hp[2].as<float4>(),
+               hp[3].as<float4>(), hp[4].as<float4>(), hp[5].as<float4>()};
+    launch_trace(lc(), o, (int)tune.trace_block, (int)tune.persistent, (int)tune.trace_blocks_per_sm, d_queue.as<u32>(),
+                 st);
+    ev(ST_TRACE, true);
+    stage_state |= 1;
+}
+
+void Engine::enq_emit() {
+    ev(ST_EMIT, false);
+    EmitOut o{slot_pos.as<float4>(), slot_pd.as<uint2>(), counts.as<u32>()};
+    launch_emit(lc(), o, (int)tune.emit_block, (int)tune.persistent, (int)tune.emit_blocks_per_sm,
+                d_queue.as<u32>() + 1, st);
+    ev(ST_EMIT, true);
+    ev(ST_EMIT_SCAN, false);
+    launch_scan(counts.as<u32>(), offsets.as<u32>(), (u64)total_emit + 1, scan_scr.p, d_ntotal.as<u32>(),
+                d_err.as<u32>(), st);
+    launch_compact(lc(), gb(), st);
+    ev(ST_EMIT_SCAN, true);
+    stage_state |= 2;
+}
+
+void Engine::enq_hash_sort() {
+    ev(ST_HASH, false);
+    cudaMemsetAsync(cell_count.p, 0, 4 * ((size_t)total_cells + 1), st);
+    launch_hash(lc(), gb(), d_ntotal.as<u32>(), max_photons, st);
+    ev(ST_HASH, true);
+    ev(ST_CELL_SCAN, false);
+    launch_scan(cell_count.as<u32>(), cell_start.as<u32>(), (u64)total_cells + 1, scan_scr.p, nullptr,
+                d_err.as<u32>(), st);
+    ev(ST_CELL_SCAN, true);
+    ev(ST_SORT, false);
+    launch_radix_sort(keys.as<u32>(), sk0.as<u32>(), sk1.as<u32>(), sv0.as<u32>(), sv1.as<u32>(), &perm,
+                      d_ntotal.as<u32>(), max_photons, key_bits, radix_scr.p, d_err.as<u32>(), st);
+    ev(ST_SORT, true);
+    ev(ST_RECORDS, false);
+    launch_sorted_records(perm, ph_pos.as<float4>(), ph_pd.as<uint2>(), d_ntotal.as<u32>(), max_photons,
+                          s_posdir.as<float4>(), s_power.as<u32>(), d_err.as<u32>(), st);
+    ev(ST_RECORDS, true);
+    stage_state |= 4;
+}
+
+void Engine::enq_gather() {
+    ev(ST_GATHER, false);
+    GatherBufs g{hp[0].as<float4>(), hp[1].as<float4>(), hp[2].as<float4>(), hp[3].as<float4>(),
+                 hp[4].as<float4>(), hp[5].as<float4>(), s_posdir.as<float4>(), s_power.as<u32>(),
+                 cell_start.as<u32>(), (u32)max_photons, flux.as<float4>(), weight.as<float>(),
+                 radiance.as<float4>()};
+    launch_gather(lc(), g, (int)tune.gather_block, st);
+    ev(ST_GATHER, true);
+}
+
+void Engine::enq_round() {
+    enq_seeds();
+    enq_trace();
+    enq_emit();
+    enq_hash_sort();
+    enq_gather();
+}
+
+void Engine::accumulate_profile() {
+    if (!profiling)
+        return;
+    for (int s = 0; s < ST__N; s++) {
+        if (!events[2 * s] || !events[2 * s + 1])
+            continue;
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, events[2 * s], events[2 * s + 1]) == cudaSuccess)
+            prof_ms[s] += ms;
+        else
+            cudaGetLastError();
+    }
+    prof_rounds++;
+}
+
+void Engine::invalidate_graph() {
+    if (st)
+        cudaStreamSynchronize(st);
+    if (gexec)
+        cudaGraphExecDestroy(gexec);
+    if (graph)
+        cudaGraphDestroy(graph);
+    if (gexec_host)
+        cudaGraphExecDestroy(gexec_host);
+    if (graph_host)
+        cudaGraphDestroy(graph_host);
+    gexec = nullptr;
+    graph = nullptr;
+    gexec_host = nullptr;
+    graph_host = nullptr;
+}
+
+void Engine::set_profiling(bool on) {
+    if (on != profiling) // re-capture so the graph carries (or drops) the event nodes
+        invalidate_graph();
+    profiling = on;
+    for (auto &m : prof_ms)
+        m = 0.0;
+    prof_rounds = 0;
+}
+
+void Engine::stage_ms(float *out) const {
+    for (int s = 0; s < ST__N; s++)
+        out[s] = prof_rounds ? (float)(prof_ms[s] / prof_rounds) : 0.0f;
+}
+
+int Engine::sync_and_check() {
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(h_pinned, d_err.p, 8, cudaMemcpyDeviceToHost));
+    uint32_t err = h_pinned[0];
+    if (err & ERR_LOOKBACK_TIMEOUT)
+        return fail(PHX_E_TIMEOUT, "a decoupled look-back wait gave up (device error flag set)");
+    if (err & ERR_NO_PHOTONS)
+        return fail(PHX_E_NO_PHOTONS, "no photon was stored in a round (renderer.cpp:117-118)");
+    return PHX_OK;
+}
+
+int Engine::read_total(uint32_t *n) {
+    CK(cudaMemcpyAsync(h_pinned, d_ntotal.p, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    *n = h_pinned[0];
+    return PHX_OK;
+}
+
+int Engine::set_seed(uint32_t seed) {
+    std::vector<uint32_t> s(sc.size(), seed);
+    CK(cudaStreamSynchronize(st));
+    CK(cudaMemcpy(d_seeds.p, s.data(), 4 * s.size(), cudaMemcpyHostToDevice));
+    return PHX_OK;
+}
+
+int Engine::scene_photon_range(uint32_t s, uint32_t *off, uint32_t *n) {
+    CK(cudaStreamSynchronize(st));
+    if (sc.size() == 1) {
+        uint32_t v[1];
+        CK(cudaMemcpy(v, d_ntotal.p, 4, cudaMemcpyDeviceToHost));
+        *off = 0;
+        *n = v[0];
+        return PHX_OK;
+    }
+    uint32_t a = 0, b = 0;
+    CK(cudaMemcpy(&a, offsets.as<u32>() + sc[s].desc.emit_base, 4, cudaMemcpyDeviceToHost));
+    uint32_t next = s + 1 < sc.size() ? sc[s + 1].desc.emit_base : total_emit;
+    CK(cudaMemcpy(&b, offsets.as<u32>() + next, 4, cudaMemcpyDeviceToHost));
+    *off = a;
+    *n = b - a;
+    return PHX_OK;
+}
+
+int Engine::plain_round() {
+    enq_seeds();
+    enq_trace();
+    enq_emit();
+    // renderer.cpp:113-118: blocking read of the stored-photon count
+    uint32_t total = 0;
+    int r = read_total(&total);
+    if (r)
+        return r;
+    for (uint32_t s = 0; s < sc.size(); s++) {
+        uint32_t off, n;
+        if ((r = scene_photon_range(s, &off, &n)))
+            return r;
+        if (n == 0)
+            return fail(PHX_E_NO_PHOTONS, "no photon hit (renderer.cpp:117-118)");
+        sc[s].n_photons_last = n;
+    }
+    enq_hash_sort();
+    enq_gather();
+    r = sync_and_check(); // renderer.cpp:160 queue.finish()
+    if (r)
+        return r;
+    accumulate_profile();
+    for (auto &s : sc) {
+        s.rounds++;
+        s.total_emitted += s.prm.photons_per_round;
+    }
+    return PHX_OK;
+}
+
+// Captures one round (optionally without the device-side seed step) into an executable graph.
+int Engine::capture(bool with_seeds, cudaGraph_t *g, cudaGraphExec_t *ge) {
+    CK(cudaStreamSynchronize(st));
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    capturing = true;
+    if (with_seeds)
+        enq_seeds();
+    enq_trace();
+    enq_emit();
+    enq_hash_sort();
+    enq_gather();
+    capturing = false;
+    cudaError_t e = cudaStreamEndCapture(st, g);
+    if (e != cudaSuccess) {
+        *g = nullptr;
+        return fail(PHX_E_CUDA, std::string("stream capture failed: ") + cudaGetErrorString(e));
+    }
+    CK(cudaGraphInstantiate(ge, *g, 0));
+    return PHX_OK;
+}
+
+void Engine::count_round(uint32_t rounds) {
+    for (auto &s : sc) {
+        s.rounds += rounds;
+        s.total_emitted += (uint64_t)rounds * s.prm.photons_per_round;
+    }
+}
+
+int Engine::graph_rounds(uint32_t rounds) {
+    int r;
+    if (!gexec && (r = capture(true, &graph, &gexec)))
+        return r;
+    for (uint32_t i = 0; i < rounds; i++) {
+        CK(cudaGraphLaunch(gexec, st));
+        if (profiling) {
+            CK(cudaStreamSynchronize(st));
+            accumulate_profile();
+        }
+    }
+    r = sync_and_check();
+    if (r)
+        return r;
+    count_round(rounds);
+    for (uint32_t s = 0; s < sc.size(); s++) {
+        uint32_t off, n;
+        if ((r = scene_photon_range(s, &off, &n)))
+            return r;
+        sc[s].n_photons_last = n;
+    }
+    return PHX_OK;
+}
+
+int Engine::seeded_round(uint32_t seed) {
+    int r;
+    if (!gexec_host && (r = capture(false, &graph_host, &gexec_host)))
+        return r;
+    if (!h_seed_ring)
+        CK(cudaMallocHost((void **)&h_seed_ring, sizeof(u32) * SEED_RING * sc.size()));
+    const uint32_t slot = seed_slot++ % SEED_RING;
+    if (seed_ev[slot])
+        CK(cudaEventSynchronize(seed_ev[slot])); // the staging slot's previous copy has been consumed
+    else
+        CK(cudaEventCreateWithFlags(&seed_ev[slot], cudaEventDisableTiming));
+    u32 *h = h_seed_ring + slot * sc.size();
+    for (size_t s = 0; s < sc.size(); s++)
+        h[s] = seed;
+    CK(cudaMemcpyAsync(d_seeds.p, h, sizeof(u32) * sc.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaEventRecord(seed_ev[slot], st));
+    CK(cudaGraphLaunch(gexec_host, st));
+    count_round(1);
+    return PHX_OK;
+}
+
+int Engine::set_alpha(float alpha) {
+    CK(cudaStreamSynchronize(st));
+    for (auto &s : sc) {
+        s.desc.alpha = alpha;
+        s.prm.sppm_alpha = alpha;
+    }
+    std::vector<SceneDesc> d(sc.size());
+    for (size_t i = 0; i < sc.size(); i++)
+        d[i] = sc[i].desc;
+    CK(cudaMemcpy(d_desc.p, d.data(), sizeof(SceneDesc) * d.size(), cudaMemcpyHostToDevice));
+    return PHX_OK;
+}
+
+int Engine::set_n_photons(uint32_t n) {
+    if (sc.size() != 1)
+        return fail(PHX_E_UNSUPPORTED, "photon injection is only available on single-scene contexts");
+    if (n > max_photons)
+        return fail(PHX_E_INVALID, "n_photons exceeds the photon buffer (photons_per_round * max_bounces)");
+    CK(cudaStreamSynchronize(st));
+    CK(cudaMemcpy(d_ntotal.p, &n, 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(offsets.as<u32>() + total_emit, &n, 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(cell_start.as<u32>() + total_cells, &n, 4, cudaMemcpyHostToDevice));
+    sc[0].n_photons_last = n;
+    stage_state |= 2;
+    return PHX_OK;
+}
+
+namespace {
+struct BufDesc {
+    size_t esize;   // logical element size (reference layout)
+    uint64_t count; // logical elements
+};
+} // namespace
+
+int Engine::read_buffer(uint32_t s, int which, void *dst, uint64_t off, uint64_t bytes) {
+    if (s >= sc.size())
+        return fail(PHX_E_INVALID, "scene index out of range");
+    if (!dst && bytes)
+        return fail(PHX_E_INVALID, "null destination");
+    const SceneDesc &d = sc[s].desc;
+    uint32_t poff = 0, pn = 0;
+    int r;
+    if (which >= PHX_BUF_PHOTON_POS && which <= PHX_BUF_SORTED_DIR && which != PHX_BUF_CELL_COUNT)
+        if ((r = scene_photon_range(s, &poff, &pn)))
+            return r;
+    if (which == PHX_BUF_SORT_PERM && (r = scene_photon_range(s, &poff, &pn)))
+        return r;
+    CK(cudaStreamSynchronize(st));
+    BufDesc bd{0, 0};
+    switch (which) {
+    case PHX_BUF_HP_POS: case PHX_BUF_HP_NORMAL: case PHX_BUF_HP_THROUGHPUT: case PHX_BUF_HP_BASE_COLOR:
+    case PHX_BUF_HP_DIRECT: case PHX_BUF_HP_EMISSION: case PHX_BUF_FLUX: case PHX_BUF_RADIANCE:
+        bd = {16, d.n_pixels};
+        break;
+    case PHX_BUF_PHOTON_WEIGHT:
+        bd = {4, d.n_pixels};
+        break;
+    case PHX_BUF_PHOTON_POS: case PHX_BUF_SORTED_POS:
+        bd = {16, pn};
+        break;
+    case PHX_BUF_PHOTON_POWER: case PHX_BUF_PHOTON_DIR: case PHX_BUF_PHOTON_HASH: case PHX_BUF_SORTED_POWER:
+    case PHX_BUF_SORTED_DIR: case PHX_BUF_SORT_PERM:
+        bd = {4, pn};
+        break;
+    case PHX_BUF_CELL_COUNT: case PHX_BUF_CELL_START: case PHX_BUF_CELL_END:
+        bd = {4, d.n_cells};
+        break;
+    case PHX_BUF_EMIT_COUNT:
+        bd = {4, d.n_emit};
+        break;
+    case PHX_BUF_BVH_NODES:
+        bd = {sizeof(phx_bvh_node), sc[s].nodes.size()};
+        break;
+    default:
+        return fail(PHX_E_INVALID, "unknown buffer id");
+    }
+    if (off + bytes > bd.esize * bd.count)
+        return fail(PHX_E_INVALID, "read past the end of the buffer");
+    if (bytes == 0)
+        return PHX_OK;
+    const uint64_t e0 = off / bd.esize, e1 = (off + bytes + bd.esize - 1) / bd.esize, ne = e1 - e0;
+    std::vector<uint8_t> tmp(ne * bd.esize);
+    auto dcopy = [&](const void *src, size_t b) -> int {
+        CK(cudaMemcpy(tmp.data(), src, b, cudaMemcpyDeviceToHost));
+        return PHX_OK;
+    };
+    auto fetch32 = [&](const u32 *src, std::vector<uint32_t> &v) -> int {
+        v.resize(ne);
+        CK(cudaMemcpy(v.data(), src, 4 * ne, cudaMemcpyDeviceToHost));
+        return PHX_OK;
+    };
+    std::vector<uint32_t> v;
+    std::vector<uint2> v2;
+    std::vector<float4> v4;
+    switch (which) {
+    case PHX_BUF_HP_POS: case PHX_BUF_HP_NORMAL: case PHX_BUF_HP_THROUGHPUT: case PHX_BUF_HP_BASE_COLOR:
+    case PHX_BUF_HP_DIRECT: case PHX_BUF_HP_EMISSION:
+        r = dcopy(hp[which].as<float4>() + d.pixel_base + e0, 16 * ne);
+        break;
+    case PHX_BUF_FLUX:
+        r = dcopy(flux.as<float4>() + d.pixel_base + e0, 16 * ne);
+        break;
+    case PHX_BUF_RADIANCE:
+        r = dcopy(radiance.as<float4>() + d.pixel_base + e0, 16 * ne);
+        break;
+    case PHX_BUF_PHOTON_WEIGHT:
+        r = dcopy(weight.as<float>() + d.pixel_base + e0, 4 * ne);
+        break;
+    case PHX_BUF_PHOTON_POS:
+        r = dcopy(ph_pos.as<float4>() + poff + e0, 16 * ne);
+        break;
+    case PHX_BUF_PHOTON_POWER: case PHX_BUF_PHOTON_DIR:
+        v2.resize(ne);
+        CK(cudaMemcpy(v2.data(), ph_pd.as<uint2>() + poff + e0, 8 * ne, cudaMemcpyDeviceToHost));
+        for (uint64_t i = 0; i < ne; i++)
+            ((uint32_t *)tmp.data())[i] = which == PHX_BUF_PHOTON_POWER ? v2[i].x : v2[i].y;
+        r = PHX_OK;
+        break;
+    case PHX_BUF_PHOTON_HASH:
+        if (!(r = fetch32(keys.as<u32>() + poff + e0, v)))
+            for (uint64_t i = 0; i < ne; i++)
+                ((uint32_t *)tmp.data())[i] = v[i] - d.cell_base;
+        break;
+    case PHX_BUF_CELL_COUNT:
+        r = dcopy(cell_count.as<u32>() + d.cell_base + e0, 4 * ne);
+        break;
+    case PHX_BUF_CELL_START: case PHX_BUF_CELL_END:
+        if (!(r = fetch32(cell_start.as<u32>() + d.cell_base + e0 + (which == PHX_BUF_CELL_END ? 1 : 0), v)))
+            for (uint64_t i = 0; i < ne; i++)
+                ((uint32_t *)tmp.data())[i] = v[i] - poff;
+        break;
+    case PHX_BUF_SORTED_POS: case PHX_BUF_SORTED_DIR:
+        v4.resize(ne);
+        CK(cudaMemcpy(v4.data(), s_posdir.as<float4>() + poff + e0, 16 * ne, cudaMemcpyDeviceToHost));
+        for (uint64_t i = 0; i < ne; i++) {
+            if (which == PHX_BUF_SORTED_POS) {
+                float q[4] = {v4[i].x, v4[i].y, v4[i].z, 0.0f};
+                std::memcpy(tmp.data() + 16 * i, q, 16);
+            } else {
+                std::memcpy(tmp.data() + 4 * i, &v4[i].w, 4);
+            }
+        }
+        r = PHX_OK;
+        break;
+    case PHX_BUF_SORTED_POWER:
+        r = dcopy(s_power.as<u32>() + poff + e0, 4 * ne);
+        break;
+    case PHX_BUF_EMIT_COUNT:
+        r = dcopy(counts.as<u32>() + d.emit_base + e0, 4 * ne);
+        break;
+    case PHX_BUF_BVH_NODES:
+        std::memcpy(tmp.data(), sc[s].nodes.data() + e0, sizeof(phx_bvh_node) * ne);
+        r = PHX_OK;
+        break;
+    case PHX_BUF_SORT_PERM:
+        if (!(r = fetch32(perm + poff + e0, v)))
+            for (uint64_t i = 0; i < ne; i++)
+                ((uint32_t *)tmp.data())[i] = v[i] - poff;
+        break;
+    default:
+        return fail(PHX_E_INVALID, "unknown buffer id");
+    }
+    if (r)
+        return r;
+    std::memcpy(dst, tmp.data() + (off - e0 * bd.esize), bytes);
+    return PHX_OK;
+}
+
+int Engine::write_buffer(uint32_t s, int which, const void *src, uint64_t off, uint64_t bytes) {
+    if (sc.size() != 1 || s != 0)
+        return fail(PHX_E_UNSUPPORTED, "buffer writes are only available on single-scene contexts");
+    if (!src && bytes)
+        return fail(PHX_E_INVALID, "null source");
+    const SceneDesc &d = sc[0].desc;
+    CK(cudaStreamSynchronize(st));
+    auto put = [&](void *base, size_t cap) -> int {
+        if (off + bytes > cap)
+            return fail(PHX_E_INVALID, "write past the end of the buffer");
+        CK(cudaMemcpy((char *)base + off, src, bytes, cudaMemcpyHostToDevice));
+        return PHX_OK;
+    };
+    const size_t P = d.n_pixels, N = max_photons;
+    switch (which) {
+    case PHX_BUF_HP_POS: case PHX_BUF_HP_NORMAL: case PHX_BUF_HP_THROUGHPUT: case PHX_BUF_HP_BASE_COLOR:
+    case PHX_BUF_HP_DIRECT: case PHX_BUF_HP_EMISSION:
+        stage_state |= 1;
+        return put(hp[which].p, 16 * P);
+    case PHX_BUF_FLUX:
+        return put(flux.p, 16 * P);
+    case PHX_BUF_RADIANCE:
+        return put(radiance.p, 16 * P);
+    case PHX_BUF_PHOTON_WEIGHT:
+        return put(weight.p, 4 * P);
+    case PHX_BUF_PHOTON_POS:
+        return put(ph_pos.p, 16 * N);
+    case PHX_BUF_SORTED_POWER:
+        stage_state |= 4;
+        return put(s_power.p, 4 * N);
+    case PHX_BUF_CELL_START:
+        stage_state |= 4;
+        return put(cell_start.p, 4 * (size_t)d.n_cells);
+    case PHX_BUF_PHOTON_POWER: case PHX_BUF_PHOTON_DIR: case PHX_BUF_SORTED_POS: case PHX_BUF_SORTED_DIR: {
+        const bool sorted = which == PHX_BUF_SORTED_POS || which == PHX_BUF_SORTED_DIR;
+        const size_t es = which == PHX_BUF_SORTED_POS ? 16 : 4;
+        if (off % es || bytes % es)
+            return fail(PHX_E_INVALID, "unaligned partial write");
+        const uint64_t e0 = off / es, ne = bytes / es;
+        if (e0 + ne > N)
+            return fail(PHX_E_INVALID, "write past the end of the buffer");
+        if (sorted) {
+            std::vector<float4> v(ne);
+            CK(cudaMemcpy(v.data(), s_posdir.as<float4>() + e0, 16 * ne, cudaMemcpyDeviceToHost));
+            for (uint64_t i = 0; i < ne; i++) {
+                if (which == PHX_BUF_SORTED_POS) {
+                    const float *q = (const float *)src + 4 * i;
+                    v[i].x = q[0];
+                    v[i].y = q[1];
+                    v[i].z = q[2];
+                } else {
+                    std::memcpy(&v[i].w, (const uint32_t *)src + i, 4);
+                }
+            }
+            CK(cudaMemcpy(s_posdir.as<float4>() + e0, v.data(), 16 * ne, cudaMemcpyHostToDevice));
+            stage_state |= 4;
+        } else {
+            std::vector<uint2> v(ne);
+            CK(cudaMemcpy(v.data(), ph_pd.as<uint2>() + e0, 8 * ne, cudaMemcpyDeviceToHost));
+            for (uint64_t i = 0; i < ne; i++) {
+                uint32_t x = ((const uint32_t *)src)[i];
+                if (which == PHX_BUF_PHOTON_POWER)
+                    v[i].x = x;
+                else
+                    v[i].y = x;
+            }
+            CK(cudaMemcpy(ph_pd.as<uint2>() + e0, v.data(), 8 * ne, cudaMemcpyHostToDevice));
+        }
+        return PHX_OK;
+    }
+    default:
+        return fail(PHX_E_UNSUPPORTED, "buffer is not writable");
+    }
+}
+
+int Engine::info(uint32_t s, phx_info *o) {
+    if (s >= sc.size() || !o)
+        return fail(PHX_E_INVALID, "bad info request");
+    std::memset(o, 0, sizeof(*o));
+    const SceneSlot &S = sc[s];
+    o->n_pixels = S.desc.n_pixels;
+    o->width = S.desc.width;
+    o->height = S.desc.height;
+    o->photons_per_round = S.prm.photons_per_round;
+    o->photon_buf_size = S.prm.photons_per_round * S.prm.max_photon_bounces;
+    o->bucket_count = S.desc.n_cells;
+    o->n_photons = S.n_photons_last;
+    o->n_bvh_nodes = (uint32_t)S.nodes.size();
+    o->bvh_depth = S.depth;
+    o->rounds_done = S.rounds;
+    o->total_photons_emitted = S.total_emitted;
+    o->hash = S.hash;
+    o->sort_passes = radix_passes(key_bits);
+    // seeds, trace, emit, count scan, compaction, hash, cell scan, 3 per sort pass, records, gather
+    o->kernels_per_round = 9 + 3 * o->sort_passes;
+    CK(cudaStreamSynchronize(st));
+    uint32_t v[2] = {0, 0};
+    CK(cudaMemcpy(&v[0], d_ovf.p, 4, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&v[1], d_err.p, 4, cudaMemcpyDeviceToHost));
+    o->stack_overflows = v[0];
+    o->error_flags = v[1];
+    return PHX_OK;
+}
+
+int Engine::image(uint32_t s, float exposure, int tonemap, uint64_t total_photons, uint32_t rounds, float *rgb,
+                  uint8_t *ldr) {
+    if (s >= sc.size())
+        return fail(PHX_E_INVALID, "scene index out of range");
+    const SceneSlot &S = sc[s];
+    if (total_photons == 0 && rounds == 0) {
+        total_photons = S.total_emitted;
+        rounds = S.rounds;
+    }
+    const uint32_t n = S.desc.n_pixels;
+    int r;
+    if (img_rgb.bytes < (size_t)n * 12 && (r = img_rgb.alloc((size_t)n * 12)))
+        return r;
+    if (img_ldr.bytes < (size_t)n * 3 && (r = img_ldr.alloc((size_t)n * 3)))
+        return r;
+    float inv_ph = total_photons > 0 ? 1.0f / (float)total_photons : 0.0f; // output.cpp:56-57
+    float inv_r = rounds > 0 ? 1.0f / (float)rounds : 0.0f;
+    launch_image(flux.as<float4>() + S.desc.pixel_base, radiance.as<float4>() + S.desc.pixel_base, n, exposure, tonemap,
+                 inv_ph, inv_r, rgb ? img_rgb.as<float>() : nullptr, ldr ? img_ldr.as<uint8_t>() : nullptr, st);
+    if (rgb)
+        CK(cudaMemcpyAsync(rgb, img_rgb.p, (size_t)n * 12, cudaMemcpyDeviceToHost, st));
+    if (ldr)
+        CK(cudaMemcpyAsync(ldr, img_ldr.p, (size_t)n * 3, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return PHX_OK;
+}
+
+} // namespace phx

@@ -1,0 +1,119 @@
+// engine.hpp — device memory layout and stage orchestration for one or many scenes.
+//
+// HBM layout (all scenes concatenated in scene order, see DESIGN.md for sizes):
+//   per pixel    hit point SoA: 6 x float4 (pos, normal, throughput, base colour, direct,
+//                emission) + SPPM state flux float4, weight f32, radiance float4   (132 B)
+//   per path     stored-photon count u32, exclusive offset u32
+//   per slot     photon slot (max_bounces per path, slot-major): float4 pos + uint2 (rgbe, oct)
+//   per photon   canonical float4 pos + uint2, u32 key, sort keys/values, cell-ordered
+//                float4 {x,y,z,dir bits} + u32 power
+//   per cell     count u32, start u32 (one extra trailing cell holds the total)
+// A context is an engine with one scene; a batch is an engine with many, every stage of every
+// scene in one launch.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "host.hpp"
+#include "kernels.hpp"
+
+namespace phx {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    int alloc(size_t b);
+    void release();
+    template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+struct SceneSlot {
+    phx_params prm{};
+    phx_photon_hash_data hash{};
+    std::vector<phx_bvh_node> nodes;
+    uint32_t depth = 0;
+    uint32_t n_tris = 0;
+    std::vector<DevBuf> bufs;
+    SceneDesc desc{};
+    uint64_t total_emitted = 0;
+    uint32_t rounds = 0;
+    uint32_t n_photons_last = 0;
+};
+
+enum Stage { ST_SEEDS = 0, ST_TRACE, ST_EMIT, ST_EMIT_SCAN, ST_HASH, ST_CELL_SCAN, ST_SORT, ST_RECORDS, ST_GATHER, ST__N };
+
+class Engine {
+  public:
+    ~Engine();
+    int create(const phx_scene *scenes, const phx_params *params, uint32_t n, int device);
+
+    // enqueue (no host sync)
+    void enq_seeds();
+    void enq_trace();
+    void enq_emit();
+    void enq_hash_sort();
+    void enq_gather();
+    void enq_round();
+
+    int plain_round();                // reference form: two host syncs per round
+    int graph_rounds(uint32_t rounds); // captured round replayed `rounds` times
+    int seeded_round(uint32_t seed);   // one replay, seed copied from pinned host memory (async)
+    int sync_and_check();
+    int set_seed(uint32_t seed);      // explicit seed for the per-stage API (all scenes)
+    int read_total(uint32_t *n);      // blocking read of the stored-photon total
+    int read_buffer(uint32_t scene, int which, void *dst, uint64_t off, uint64_t bytes);
+    int write_buffer(uint32_t scene, int which, const void *src, uint64_t off, uint64_t bytes);
+    int set_n_photons(uint32_t n);
+    int info(uint32_t scene, phx_info *out);
+    int image(uint32_t scene, float exposure, int tonemap, uint64_t total_photons, uint32_t rounds, float *rgb,
+              uint8_t *ldr);
+    int set_alpha(float alpha);
+    void set_profiling(bool on);
+    void stage_ms(float *out) const;
+    void invalidate_graph();
+
+    int device = 0;
+    cudaStream_t st = nullptr;
+    std::vector<SceneSlot> sc;
+    uint32_t total_pixels = 0, total_emit = 0, total_cells = 0;
+    uint64_t total_slots = 0, max_photons = 0;
+    uint32_t key_bits = 1;
+    phx_tuning tune{};
+    int stage_state = 0;
+
+  private:
+    LaunchCtx lc() const;
+    GridBufs gb() const;
+    int upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, uint32_t *pix, uint32_t *emit,
+                     uint32_t *cell, uint64_t *slot);
+    int scene_photon_range(uint32_t s, uint32_t *off, uint32_t *n);
+    void ev(int stage, bool end);
+    void accumulate_profile();
+
+    DevBuf d_desc, d_pix_bases, d_emit_bases, d_seeds, d_rng, d_err, d_ovf, d_queue, d_ntotal;
+    DevBuf hp[6], flux, weight, radiance;
+    DevBuf slot_pos, slot_pd, counts, offsets, ph_pos, ph_pd, keys, cell_count, cell_start;
+    DevBuf sk0, sk1, sv0, sv1, s_posdir, s_power, scan_scr, radix_scr, img_rgb, img_ldr;
+    int capture(bool with_seeds, cudaGraph_t *g, cudaGraphExec_t *ge);
+    void count_round(uint32_t rounds);
+
+    u32 *perm = nullptr;
+    u32 *h_pinned = nullptr;
+    cudaGraph_t graph = nullptr, graph_host = nullptr;
+    cudaGraphExec_t gexec = nullptr, gexec_host = nullptr;
+    static constexpr int SEED_RING = 64;
+    u32 *h_seed_ring = nullptr; // pinned staging for host-given round seeds
+    cudaEvent_t seed_ev[SEED_RING] = {};
+    uint32_t seed_slot = 0;
+    uint32_t pending_seeded = 0;
+    bool profiling = false, capturing = false;
+    cudaEvent_t events[2 * ST__N] = {};
+    double prof_ms[ST__N] = {};
+    uint32_t prof_rounds = 0;
+};
+
+extern thread_local std::string g_last_error;
+int fail(int code, const std::string &msg);
+
+} // namespace phx

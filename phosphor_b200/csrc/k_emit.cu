@@ -1,0 +1,118 @@
+// k_emit.cu — photon paths from the lights, stored at diffuse bounces
+// (kernels/emit_photons.cl:12-114).
+//
+// Canonical order instead of atomic compaction.  The reference appends each stored photon at
+// atomic_inc(n_photons) (emit_photons.cl:98), so its photon order depends on scheduling.  Here
+// path t writes its j-th stored photon to slot (j, t) of a slot array laid out slot-major
+// (slot_base + j*n_emit + t: lanes of a warp store to consecutive addresses) and its store count
+// to counts[t].  An exclusive scan of the counts then places photon (t, j) at offsets[t] + j —
+// the order a sequential run of emit_photons.cl produces — and the compaction is fused into the
+// hash kernel.  A path stores at most one photon per bounce, so max_bounces slots per path
+// always suffice, exactly like the reference's photons*max_bounces buffer (renderer.cpp:40).
+#include "dev_shading.cuh"
+#include "kernels.hpp"
+
+namespace phx {
+
+PHX_DI u32 emit_path(const SceneDesc &sc, u32 seed, u32 tid, const EmitOut &out, u32 *overflow) {
+    u32 n_out = 0;
+    const u64 stride = sc.n_emit;
+    u64 slot = sc.slot_base + tid;
+    Rng rng = pcg_seed(seed + tid);
+    float4 origin, dir, power;
+    sample_light(&rng, sc, &origin, &dir, &power);
+    IorStack ior;
+    init_ior_stack(&ior, AIR_IOR);
+    float4 throughput = f4(1.0f, 1.0f, 1.0f, 0.0f);
+    for (u32 depth = 0; depth < sc.max_bounces; depth++) {
+        Hit h;
+        bool hit = intersect(sc, origin, dir, EPS, INF, &h, overflow);
+        if (!hit)
+            return n_out;
+        SurfaceHit sh = process_hit(sc, h, origin, dir);
+        const phx_material mat = sc.materials[sh.mat_index];
+        float4 vol = white4();
+        float cur = current_ior(&ior);
+        if (cur != AIR_IOR && mat.thickness > EPS && mat.att_dist > EPS) {
+            vol = beer_lambert(f4(mat.att_color), mat.att_dist, sh.t);
+            power *= vol;
+            throughput *= vol;
+        }
+        float4 tangent, bitangent;
+        hit_frame(sc, h, sh, &tangent, &bitangent);
+        ShadingContext ctx = evaluate_material(sc, mat, sh.mat_index, sh.uvx, sh.uvy, sh.normal, tangent, bitangent);
+        if (depth >= RR_MIN_PHOTON_DEPTH) {
+            float q = fmaxf(throughput.x, fmaxf(throughput.y, throughput.z));
+            q = clampf(q, RR_MIN_Q, RR_MAX_Q);
+            if (random_float(&rng) > q)
+                return n_out;
+            float inv_q = 1.0f / q;
+            throughput *= inv_q;
+            power *= inv_q;
+        }
+        float4 view = -dir;
+        BsdfSample bs = sample_bsdf(&rng, ctx, ctx.shading_normal, sh.normal, view, &ior, sh.front_face);
+        if (bs.event == BSDF_DIFFUSE && dot(dir, sh.normal) < 0.0f) {
+            out.slot_pos[slot] = sh.position;
+            out.slot_pd[slot] = make_uint2(encode_rgbe(power), encode_oct(dir));
+            slot += stride;
+            n_out++;
+        }
+        power *= bs.throughput;
+        throughput *= bs.throughput;
+        float4 side = (dot(bs.dir, sh.normal) > 0.0f) ? sh.normal : -sh.normal;
+        origin = sh.position + bs.dir * EPS + side * EPS;
+        dir = bs.dir;
+    }
+    return n_out;
+}
+
+__global__ void __launch_bounds__(128) k_emit(LaunchCtx lc, EmitOut out) {
+    u32 gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= lc.total_emit)
+        return;
+    u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.emit_bases, lc.n_scenes, gid);
+    const SceneDesc &sc = lc.scenes[s];
+    u32 ovf = 0;
+    out.counts[gid] = emit_path(sc, __ldg(&lc.seeds[s]), gid - sc.emit_base, out, &ovf);
+    if (ovf)
+        atomicAdd(lc.overflow, ovf);
+}
+
+__global__ void __launch_bounds__(128) k_emit_persistent(LaunchCtx lc, EmitOut out, u32 *queue) {
+    const u32 lane = threadIdx.x & 31u;
+    u32 ovf = 0;
+    for (;;) {
+        u32 base = 0;
+        if (lane == 0)
+            base = atomicAdd(queue, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= lc.total_emit)
+            break;
+        u32 gid = base + lane;
+        if (gid < lc.total_emit) {
+            u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.emit_bases, lc.n_scenes, gid);
+            const SceneDesc &sc = lc.scenes[s];
+            out.counts[gid] = emit_path(sc, __ldg(&lc.seeds[s]), gid - sc.emit_base, out, &ovf);
+        }
+    }
+    if (ovf)
+        atomicAdd(lc.overflow, ovf);
+}
+
+void launch_emit(const LaunchCtx &lc, const EmitOut &out, int block, int persistent, int blocks_per_sm, u32 *queue,
+                 cudaStream_t st) {
+    if (lc.total_emit == 0)
+        return;
+    if (persistent && queue) {
+        cudaMemsetAsync(queue, 0, sizeof(u32), st);
+        int grid = g_sm_count * (blocks_per_sm > 0 ? blocks_per_sm : 8);
+        k_emit_persistent<<<grid, 128, 0, st>>>(lc, out, queue);
+    } else {
+        (void)block;
+        u32 grid = (lc.total_emit + 127) / 128;
+        k_emit<<<grid, 128, 0, st>>>(lc, out);
+    }
+}
+
+} // namespace phx

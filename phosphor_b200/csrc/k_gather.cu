@@ -1,0 +1,133 @@
+// k_gather.cu — per-pixel photon gather with the SPPM radius/flux update
+// (kernels/gather_flux.cl:5-78, gather_photon_flux in include/common/photon_hash.h:56-103), and
+// the image formation of src/renderer/output.cpp:40-83.
+//
+// Photons are read in cell order from the sorted records {x, y, z, octahedral dir bits} (16 B,
+// one load answers the radius test and the orientation test) plus the RGBE power word, which is
+// only loaded for photons inside the radius.  Each pixel accumulates its 27 cells in the
+// reference's cell order and each cell in sorted (= canonical) order, in one thread with no float
+// atomics, so the sum is deterministic and equal to the reference's sequential sum.  cell_end is
+// not materialised: the cells are contiguous, so end(h) = start(h+1).
+#include "kernels.hpp"
+
+namespace phx {
+
+PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
+    float4 ge = g.hp_emission[gpix];
+    float4 rso = g.radiance[gpix];
+    float4 r = f4(ge.x, ge.y, ge.z, 0.0f);
+    if (ge.w == 0.0f) {
+        g.radiance[gpix] = rso + r;
+        return;
+    }
+    float4 direct = g.hp_direct[gpix];
+    r.x += direct.x;
+    r.y += direct.y;
+    r.z += direct.z;
+    g.radiance[gpix] = rso + r;
+    float4 fso = g.flux[gpix];
+    float wso = g.weight[gpix];
+    const GridDev grid = sc.grid;
+    float r_sq = fso.w;
+    if (r_sq < EPS) {
+        float hx = grid.cx * 0.5f, hy = grid.cy * 0.5f, hz = grid.cz * 0.5f;
+        r_sq = hx * hx + hy * hy + hz * hz;
+    }
+    const float4 pos = g.hp_pos[gpix];
+    const float4 nrm = g.hp_normal[gpix];
+    float4 nf = zero4();
+    float found = 0.0f;
+    const u32 *cs = g.cell_start + sc.cell_base;
+    const float denom = 2.0f * r_sq;
+    for (u32 i = 0; i < 27; i++) {
+        i32 cx = (i32)(i % 3) - 1;
+        i32 cy = (i32)((i / 3) % 3) - 1;
+        i32 cz = (i32)((i / 9) % 3) - 1;
+        float px = pos.x, py = pos.y, pz = pos.z;
+        px += (float)cx * grid.cx;
+        py += (float)cy * grid.cy;
+        pz += (float)cz * grid.cz;
+        u32 h = get_hash(px, py, pz, grid);
+        if (h == 0)
+            continue;
+        u32 start = min(__ldg(&cs[h]), g.n_cap);
+        u32 end = min(__ldg(&cs[h + 1]), g.n_cap);
+        for (u32 k = start; k < end; k++) {
+            float4 p = __ldg(&g.s_posdir[k]);
+            float dx = pos.x - p.x, dy = pos.y - p.y, dz = pos.z - p.z, dw = pos.w - 0.0f;
+            float dsq = ((dx * dx + dy * dy) + dz * dz) + dw * dw;
+            if (dsq >= r_sq)
+                continue;
+            float4 pd = decode_oct(__float_as_uint(p.w));
+            if (dot(pd, nrm) > 0.0f)
+                continue;
+            float w = GAUSS_ALPHA * (1.0f - (1.0f - pm_expf((-GAUSS_BETA) * dsq / denom)) / GAUSS_DENOM);
+            nf += w * decode_rgbe(__ldg(&g.s_power[k]));
+            found += w;
+        }
+    }
+    if (found > 0.0f) {
+        float nw = wso + sc.alpha * found;
+        float ratio = nw / (wso + found);
+        float nr = r_sq * ratio;
+        float4 albedo = g.hp_base_color[gpix];
+        float4 contribution = g.hp_throughput[gpix] * (albedo / PI) * nf;
+        float4 temp = (fso + contribution) * ratio;
+        g.flux[gpix] = f4(temp.x, temp.y, temp.z, nr);
+        g.weight[gpix] = nw;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_gather(LaunchCtx lc, GatherBufs g) {
+    u32 gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= lc.total_pixels)
+        return;
+    u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gid);
+    gather_pixel(lc.scenes[s], gid, g);
+}
+
+void launch_gather(const LaunchCtx &lc, const GatherBufs &g, int block, cudaStream_t st) {
+    if (lc.total_pixels == 0)
+        return;
+    (void)block;
+    k_gather<<<(lc.total_pixels + 127) / 128, 128, 0, st>>>(lc, g);
+}
+
+// output.cpp:40-50 tone_map and :52-83 apply_tonemap, before/after u8 quantisation
+__global__ void k_image(const float4 *flux, const float4 *radiance, u32 n, float exposure, int tonemap,
+                        float inv_photons, float inv_rounds, float *rgb, uint8_t *ldr) {
+    u32 p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n)
+        return;
+    float4 f = flux[p], rad = radiance[p];
+    float area = PI * f.w;
+    float ir = 0.0f, ig = 0.0f, ib = 0.0f;
+    if (area > 0.0f) {
+        float per = inv_photons / area;
+        ir = f.x * per;
+        ig = f.y * per;
+        ib = f.z * per;
+    }
+    float c[3] = {rad.x * inv_rounds + ir, rad.y * inv_rounds + ig, rad.z * inv_rounds + ib};
+    for (int k = 0; k < 3; k++) {
+        float x = c[k] * exposure;
+        float out = x;
+        if (tonemap)
+            out = (x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f);
+        out = pm_powf(out, 1.0f / 2.2f);
+        out = clampf(out, 0.0f, 1.0f);
+        if (rgb)
+            rgb[(size_t)p * 3 + k] = out;
+        if (ldr)
+            ldr[(size_t)p * 3 + k] = (uint8_t)(out * 255.0f);
+    }
+}
+
+void launch_image(const float4 *flux, const float4 *radiance, u32 n, float exposure, int tonemap, float inv_photons,
+                  float inv_rounds, float *rgb, uint8_t *ldr, cudaStream_t st) {
+    if (n == 0)
+        return;
+    k_image<<<(n + 255) / 256, 256, 0, st>>>(flux, radiance, n, exposure, tonemap, inv_photons, inv_rounds, rgb, ldr);
+}
+
+} // namespace phx

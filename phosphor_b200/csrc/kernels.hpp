@@ -1,0 +1,94 @@
+// kernels.hpp — host-side launchers of the SPPM device kernels (one translation unit each).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dev_scene.cuh"
+
+namespace phx {
+
+// Global index spaces of an engine: pixels, photon paths, photon slots and grid cells of all
+// scenes concatenated in scene order.  bases arrays hold n_scenes+1 prefix offsets.
+struct LaunchCtx {
+    const SceneDesc *scenes; // device array
+    u32 n_scenes;
+    const u32 *pix_bases;    // device
+    const u32 *emit_bases;   // device
+    u32 total_pixels;
+    u32 total_emit;
+    const u32 *seeds;        // device, one round seed per scene
+    u32 *err;                // device error word
+    u32 *overflow;           // device traversal-overflow counter
+};
+
+struct TraceOut {
+    float4 *pos, *normal, *throughput, *base_color, *direct, *emission;
+};
+
+// Persistent work queue (lane refill): a device counter the kernel drains.
+void launch_trace(const LaunchCtx &lc, const TraceOut &out, int block, int persistent, int blocks_per_sm,
+                  u32 *queue, cudaStream_t st);
+
+struct EmitOut {
+    float4 *slot_pos;
+    uint2 *slot_pd; // (rgbe power, octahedral direction)
+    u32 *counts;    // per photon path (global emit index)
+};
+void launch_emit(const LaunchCtx &lc, const EmitOut &out, int block, int persistent, int blocks_per_sm, u32 *queue,
+                 cudaStream_t st);
+
+// grid build
+struct GridBufs {
+    const u32 *counts;   // per photon path
+    const u32 *offsets;  // exclusive scan of counts, total_emit+1 entries
+    const float4 *slot_pos;
+    const uint2 *slot_pd;
+    float4 *ph_pos;      // canonical photons
+    uint2 *ph_pd;
+    u32 *keys;           // composite cell key per canonical photon
+    u32 *cell_count;     // total_cells+1
+};
+void launch_compact(const LaunchCtx &lc, const GridBufs &g, cudaStream_t st);
+void launch_hash(const LaunchCtx &lc, const GridBufs &g, const u32 *n_dev, u64 n_max, cudaStream_t st);
+
+// exclusive scan of n u32 (decoupled look-back).  total (optional) receives the sum.
+// scratch: ScanScratch sized by scan_scratch_words(n).
+size_t scan_scratch_bytes(u64 n);
+void launch_scan(const u32 *in, u32 *out, u64 n, void *scratch, u32 *total, u32 *err, cudaStream_t st);
+// failure-detection self-test: scan with tile 0 withheld; returns 0 ok, 2 alloc, 3 CUDA error
+int selftest_lookback_timeout(int device, u32 n, u32 *err_out);
+
+// stable LSD radix sort of (key, canonical index) by key; n read from device *n_dev (<= n_max)
+size_t radix_scratch_bytes(u64 n_max, u32 key_bits);
+u32 radix_passes(u32 key_bits);
+void launch_radix_sort(const u32 *keys_in, u32 *keys_tmp0, u32 *keys_tmp1, u32 *vals0, u32 *vals1, u32 **perm_out,
+                       const u32 *n_dev, u64 n_max, u32 key_bits, void *scratch, u32 *err, cudaStream_t st);
+
+void launch_sorted_records(const u32 *perm, const float4 *ph_pos, const uint2 *ph_pd, const u32 *n_dev, u64 n_max,
+                           float4 *s_posdir, u32 *s_power, u32 *err, cudaStream_t st);
+
+struct GatherBufs {
+    const float4 *hp_pos, *hp_normal, *hp_throughput, *hp_base_color, *hp_direct, *hp_emission;
+    const float4 *s_posdir;
+    const u32 *s_power;
+    const u32 *cell_start; // total_cells+1
+    u32 n_cap;             // photon buffer capacity: cell ranges are clamped to it
+    float4 *flux;
+    float *weight;
+    float4 *radiance;
+};
+void launch_gather(const LaunchCtx &lc, const GatherBufs &g, int block, cudaStream_t st);
+
+// image formation (output.cpp:52-83) for one scene's pixel range
+void launch_image(const float4 *flux, const float4 *radiance, u32 n, float exposure, int tonemap, float inv_photons,
+                  float inv_rounds, float *rgb, uint8_t *ldr, cudaStream_t st);
+
+// per-scene round seeds: seeds[s] = random_u32(&state[s])
+void launch_next_seeds(u32 *state, u32 *seeds, u32 n, cudaStream_t st);
+
+// SM count of the current device (set by init_kernels, called once per engine outside capture)
+extern int g_sm_count;
+void init_kernels(int device);
+
+} // namespace phx

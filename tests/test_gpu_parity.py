@@ -1,0 +1,341 @@
+"""Parity of the sm_100a kernels with the oracle, stage by stage and end to end (needs a GPU).
+
+Every comparison runs the CUDA path through the C ABI (libphx.so) and the CPU restatement of the
+reference (oracle/) on the same scene, seeds and inputs.  Integer results (cell keys, per-cell
+counts, cell starts, the scatter permutation, photon codes) must be bit-exact; float results are
+compared for exact equality first and must in any case agree within REL_TOL = 1e-4 relative.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle as O
+import phosphor_b200 as P
+from phosphor_b200 import _capi as A
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-4  # float tolerance of the parity contract (hit points, photons, flux)
+
+SCENES = {
+    # name: (kind, detail, width, height, photons, max_bounces, grid_res)
+    "cornell": (A.PHX_SCENE_CORNELL, 0, 64, 64, 1 << 14, 8, 50),
+    "caustic": (A.PHX_SCENE_CAUSTIC, 0, 48, 40, 1 << 13, 12, 50),
+    "atrium": (A.PHX_SCENE_ATRIUM, 16, 48, 27, 1 << 13, 16, 64),
+}
+
+
+def make(name, seed=1, **over):
+    kind, detail, w, h, ph, mb, g = SCENES[name]
+    scene = P.SceneData.generate(kind, seed=seed, width=w, height=h, detail=detail)
+    args = P.ArgsList(width=w, height=h, photons_per_round=ph, max_photon_bounces=mb, grid_res=g, seed=seed,
+                      direct_samples=16)
+    for k, v in over.items():
+        setattr(args, k, v)
+    return scene, args
+
+
+def assert_close(name, got, want, rel=REL_TOL):
+    got = np.asarray(got, np.float64)
+    want = np.asarray(want, np.float64)
+    assert got.shape == want.shape, name
+    exact = np.mean(got == want)
+    err = np.abs(got - want) / np.maximum(np.abs(want), 1e-30)
+    bad = (err > rel) & (np.abs(got - want) > 1e-30)
+    assert not bad.any(), f"{name}: {bad.sum()} of {bad.size} values beyond {rel} (exact fraction {exact:.6f})"
+    return exact
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_trace_rays_parity(name):
+    scene, args = make(name)
+    o = O.Oracle(scene)
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        seed = 0x9E3779B9
+        r.trace_rays(seed)
+        got = np.stack([r.read(b) for b in ["HP_POS", "HP_NORMAL", "HP_THROUGHPUT", "HP_BASE_COLOR", "HP_DIRECT",
+                                             "HP_EMISSION"]], axis=1)
+        assert r.info().stack_overflows == 0
+    want = o.trace(args.width, args.height, seed, args.direct_samples)
+    exact = assert_close(f"{name} hit points", got, want)
+    assert exact == 1.0, f"{name}: hit points not bit-exact ({exact})"
+    assert (want[:, 5, 3] == 1.0).mean() > 0.3  # many pixels found a diffuse hit point
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_emit_photons_parity(name):
+    scene, args = make(name)
+    o = O.Oracle(scene)
+    seed = 12345
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        n = r.emit_photons(seed)
+        counts = r.read("EMIT_COUNT")
+        pos, power, dirs = r.read("PHOTON_POS"), r.read("PHOTON_POWER"), r.read("PHOTON_DIR")
+    ocounts, opos, opower, odir = o.emit(0, args.photons_per_round, args.max_photon_bounces, seed)
+    assert n == len(opos) > 0
+    assert np.array_equal(counts, ocounts)
+    assert np.array_equal(power, opower)
+    assert np.array_equal(dirs, odir)
+    exact = assert_close(f"{name} photon positions", pos, opos)
+    assert exact == 1.0
+
+
+def inject_photons(r, pos, power, dirs):
+    r.write("PHOTON_POS", np.ascontiguousarray(pos, np.float32))
+    r.write("PHOTON_POWER", np.ascontiguousarray(power, np.uint32))
+    r.write("PHOTON_DIR", np.ascontiguousarray(dirs, np.uint32))
+    r.set_n_photons(len(pos))
+
+
+@pytest.mark.parametrize("name", ["cornell", "caustic"])
+def test_hash_scan_scatter_bit_exact(name):
+    scene, args = make(name)
+    o = O.Oracle(scene)
+    _, pos, power, dirs = o.emit(0, args.photons_per_round, args.max_photon_bounces, 777)
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        inject_photons(r, pos, power, dirs)
+        r.hash_and_sort_photons()
+        info = r.info()
+        got = {b: r.read(b) for b in ["PHOTON_HASH", "CELL_COUNT", "CELL_START", "CELL_END", "SORTED_POS",
+                                      "SORTED_POWER", "SORTED_DIR", "SORT_PERM"]}
+    hd = bytes(info.hash)
+    keys, counts = O.hash_photons(pos, hd, info.bucket_count)
+    start = O.scan(counts)
+    spos, spow, sdir, end, perm = O.scatter(pos, power, dirs, keys, start)
+    assert np.array_equal(got["PHOTON_HASH"], keys)
+    assert np.array_equal(got["CELL_COUNT"], counts)
+    assert np.array_equal(got["CELL_START"], start)
+    assert np.array_equal(got["CELL_END"], end)
+    assert np.array_equal(got["SORT_PERM"], perm)
+    assert np.array_equal(got["SORTED_POS"].view(np.uint32), spos.view(np.uint32))
+    assert np.array_equal(got["SORTED_POWER"], spow)
+    assert np.array_equal(got["SORTED_DIR"], sdir)
+    # property: the permutation is the stable argsort of the keys
+    assert np.array_equal(perm, np.argsort(keys, kind="stable"))
+
+
+@pytest.mark.parametrize("dist", ["uniform", "one_cell", "outside", "clustered"])
+def test_sort_large_adversarial(dist):
+    """3M photons on the largest grid (255^3 + 1 cells, 3 radix passes) against numpy."""
+    scene, args = make("cornell", grid_res=255, photons_per_round=1 << 20, max_photon_bounces=4)
+    rng = np.random.default_rng(11)
+    n = 3_000_000
+    if dist == "uniform":
+        p = rng.uniform(-0.001, 1.001, size=(n, 3))
+    elif dist == "one_cell":
+        p = np.full((n, 3), 0.5)
+    elif dist == "outside":
+        p = rng.uniform(-0.001, 1.001, size=(n, 3))
+        p[::3, 1] = 5.0  # a third of the photons outside the grid -> key 0
+    else:
+        p = 0.5 + 0.003 * rng.standard_normal(size=(n, 3))
+    pos = np.concatenate([p, np.zeros((n, 1))], axis=1).astype(np.float32)
+    power = rng.integers(0, 2**32, size=n, dtype=np.uint32)
+    dirs = np.arange(n, dtype=np.uint32)
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        inject_photons(r, pos, power, dirs)
+        r.hash_and_sort_photons()
+        info = r.info()
+        keys_g = r.read("PHOTON_HASH")
+        counts_g = r.read("CELL_COUNT")
+        start_g = r.read("CELL_START")
+        perm_g = r.read("SORT_PERM")
+        sdir_g = r.read("SORTED_DIR")
+    keys = O.get_hash(pos, bytes(info.hash))
+    assert np.array_equal(keys_g, keys)
+    counts = np.bincount(keys, minlength=info.bucket_count).astype(np.uint32)
+    assert np.array_equal(counts_g, counts)
+    start = np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.uint32)
+    assert np.array_equal(start_g, start)
+    perm = np.argsort(keys, kind="stable").astype(np.uint32)
+    assert np.array_equal(perm_g, perm)
+    assert np.array_equal(sdir_g, dirs[perm])
+
+
+@pytest.mark.parametrize("name", ["cornell", "caustic"])
+def test_gather_parity(name):
+    """gather_flux on identical inputs: hit points and sorted photons from the oracle, with a
+    non-trivial SPPM state (radius already shrunk for some pixels)."""
+    scene, args = make(name)
+    o = O.Oracle(scene)
+    hp = o.trace(args.width, args.height, 99, args.direct_samples)
+    _, pos, power, dirs = o.emit(0, args.photons_per_round, args.max_photon_bounces, 99)
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        inject_photons(r, pos, power, dirs)
+        r.hash_and_sort_photons()
+        info = r.info()
+        rng = np.random.default_rng(4)
+        npx = args.width * args.height
+        flux = np.zeros((npx, 4), np.float32)
+        r2 = (info.hash.cell_sizes.x * 0.5) ** 2 * 3
+        flux[:, 3] = np.where(rng.uniform(size=npx) < 0.5, 0.0, r2 * rng.uniform(0.2, 1.0, size=npx))
+        flux[:, :3] = rng.uniform(0, 1, size=(npx, 3))
+        weight = rng.uniform(0, 5, size=npx).astype(np.float32)
+        radiance = rng.uniform(0, 2, size=(npx, 4)).astype(np.float32)
+        names = ["HP_POS", "HP_NORMAL", "HP_THROUGHPUT", "HP_BASE_COLOR", "HP_DIRECT", "HP_EMISSION"]
+        for k, b in enumerate(names):
+            r.write(b, hp[:, k, :])
+        r.write("FLUX", flux)
+        r.write("PHOTON_WEIGHT", weight)
+        r.write("RADIANCE", radiance)
+        r.gather_flux(0.7)
+        gf, gw, gr = r.read("FLUX"), r.read("PHOTON_WEIGHT"), r.read("RADIANCE")
+        hd = bytes(info.hash)
+    keys, counts = O.hash_photons(pos, hd, info.bucket_count)
+    start = O.scan(counts)
+    spos, spow, sdir, end, _ = O.scatter(pos, power, dirs, keys, start)
+    of, ow, orad = flux.copy(), weight.copy(), radiance.copy()
+    O.gather(hp.reshape(npx, 24), spos, spow, sdir, start, end, hd, 0.7, of, ow, orad)
+    assert (ow != weight).mean() > 0.2  # photons were found for many pixels
+    for nm, g, w in (("flux", gf, of), ("weight", gw, ow), ("radiance", gr, orad)):
+        exact = assert_close(nm, g, w)
+        assert exact == 1.0, f"{nm} not bit-exact: {exact}"
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_rounds_end_to_end(name):
+    """Three full SPPM rounds (plain per-pass form) against the oracle's Renderer::run."""
+    scene, args = make(name)
+    rounds = 3
+    o = O.Oracle(scene)
+    st = o.render(args.params(), rounds, prec=0)
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        for _ in range(rounds):
+            r.round()
+        gf, gw, gr = r.read("FLUX"), r.read("PHOTON_WEIGHT"), r.read("RADIANCE")
+        inf = r.info()
+        img = r.image()
+    assert inf.total_photons_emitted == st["total"]
+    assert inf.n_photons == st["n_last"]
+    for nm, g, w in (("flux", gf, st["flux"]), ("weight", gw, st["weight"]), ("radiance", gr, st["radiance"])):
+        exact = assert_close(f"{name} {nm}", g, w)
+        assert exact == 1.0, f"{name} {nm} not bit-exact: {exact}"
+    oimg = O.image(st["flux"], st["radiance"], 0, args.exposure, False, st["total"], rounds)
+    assert np.allclose(img.reshape(-1, 3), oimg, atol=1e-6)
+
+
+def test_graph_replay_equals_plain_rounds():
+    scene, args = make("caustic")
+    with P.Renderer(args) as a, P.Renderer(args) as b:
+        a.set_scene(scene)
+        b.set_scene(scene)
+        for _ in range(4):
+            a.round()
+        b.iterate(2)
+        b.iterate(2)
+        for buf in ["FLUX", "PHOTON_WEIGHT", "RADIANCE", "SORTED_POS", "CELL_START"]:
+            assert np.array_equal(a.read(buf).view(np.uint32), b.read(buf).view(np.uint32)), buf
+        assert a.info().total_photons_emitted == b.info().total_photons_emitted
+
+
+def test_batch_equals_single_scenes():
+    specs = [("cornell", dict(photons_per_round=1 << 13, sppm_alpha=0.62, seed=3)),
+             ("caustic", dict(photons_per_round=1 << 12, sppm_alpha=0.75, seed=4)),
+             ("atrium", dict(photons_per_round=1 << 12, sppm_alpha=0.7, seed=5))]
+    made = [make(n, **kw) for n, kw in specs]
+    rounds = 3
+    batch = P.Batch([s for s, _ in made], [a for _, a in made])
+    batch.iterate(rounds, graph=True)
+    for i, (scene, args) in enumerate(made):
+        with P.Renderer(args) as r:
+            r.set_scene(scene)
+            for _ in range(rounds):
+                r.round()
+            for buf in ["FLUX", "PHOTON_WEIGHT", "RADIANCE"]:
+                assert np.array_equal(batch.read(i, buf).view(np.uint32), r.read(buf).view(np.uint32)), (i, buf)
+            assert np.array_equal(batch.read(i, "SORT_PERM"), r.read("SORT_PERM"))
+    batch.close()
+
+
+def test_image_formation_matches_output_cpp():
+    scene, args = make("cornell")
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        r.iterate(2)
+        f, rad = r.read("FLUX"), r.read("RADIANCE")
+        inf = r.info()
+        for tm in (False, True):
+            img = r.image(tonemap=tm)
+            want = O.image(f, rad, 0, args.exposure, tm, inf.total_photons_emitted, inf.rounds_done)
+            assert np.allclose(img.reshape(-1, 3), want, atol=1e-6)
+        u8 = r.image_u8()
+        assert u8.dtype == np.uint8 and u8.shape == (args.height, args.width, 3)
+
+
+def _scene_from_arrays(tris, mats, lights, camera):
+    sc = A.Scene()
+    sc.triangles = tris.ctypes.data_as(C.POINTER(A.Triangle))
+    sc.n_triangles = len(tris)
+    sc.materials = mats.ctypes.data_as(C.POINTER(A.Material))
+    sc.n_materials = len(mats)
+    sc.emissive_triangles = tris.ctypes.data_as(C.POINTER(A.Triangle))
+    sc.n_emissive_triangles = len(tris)
+    sc.lights = lights.ctypes.data_as(C.POINTER(A.Light))
+    sc.n_lights = len(lights)
+    sc.camera = camera
+    return P.SceneData(sc, keep=(tris, mats, lights))
+
+
+def test_no_photon_hit_is_a_status():
+    """An emitter that faces away from all geometry stores nothing: the reference traps
+    (renderer.cpp:117-118); here emit_photons returns PHX_E_NO_PHOTONS."""
+    base = P.SceneData.generate(A.PHX_SCENE_CORNELL, seed=1, width=16, height=16)
+    t = base.triangles()[:2].copy()  # the floor quad, y = 0, normal +y
+    lt = t.copy()
+    for k in ("v0", "v1", "v2"):
+        lt[k]["y"] = -1.0  # light quad below the floor, facing down
+    for k in ("n0", "n1", "n2"):
+        lt[k]["y"] = -1.0
+    tris = np.concatenate([t, lt])
+    tris["mat_index"][:] = 0
+    mats = base.materials()[:1].copy()
+    lights = np.zeros(1, dtype=base.lights().dtype)
+    lights[0] = base.lights()[0]
+    aux = lights[0]["aux"]
+    aux_u = np.array([0xFFFFFFFF, 2, 2], np.uint32).view(np.float32)
+    aux["x"], aux["y"], aux["z"] = aux_u
+    scene = _scene_from_arrays(tris, mats, lights, base.scene.camera)
+    args = P.ArgsList(width=16, height=16, photons_per_round=4096, max_photon_bounces=4, grid_res=8)
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        with pytest.raises(P.PhxError) as e:
+            r.emit_photons(5)
+        assert e.value.code == A.PHX_E_NO_PHOTONS
+
+
+def test_state_and_argument_errors():
+    scene, args = make("cornell")
+    lib = A.load()
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        with pytest.raises(P.PhxError) as e:
+            r.hash_and_sort_photons()
+        assert e.value.code == A.PHX_E_STATE
+        buf = np.zeros(4, np.float32)
+        assert lib.phx_read_buffer(r.ctx, 99, buf.ctypes.data, 0, 16) == A.PHX_E_INVALID
+        assert lib.phx_read_buffer(r.ctx, A.BUF["FLUX"], buf.ctypes.data, 10**9, 16) == A.PHX_E_INVALID
+        assert lib.phx_set_n_photons(r.ctx, 2**31) == A.PHX_E_INVALID
+        t = r.tuning()
+        t.trace_block = 33
+        assert lib.phx_set_tuning(r.ctx, C.byref(t)) == A.PHX_E_INVALID
+
+
+def test_lookback_wait_gives_up_with_a_status():
+    """Failure detection without a fault: a scan whose tile 0 never publishes must time out,
+    report PHX_E_TIMEOUT and leave the device usable."""
+    lib = A.load()
+    flags = C.c_uint32()
+    assert lib.phx_selftest_lookback_timeout(0, 1 << 16, C.byref(flags)) == A.PHX_E_TIMEOUT
+    assert flags.value & 1
+    scene, args = make("cornell")  # the context still works afterwards
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        r.iterate(1)
+        assert r.info().error_flags == 0
