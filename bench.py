@@ -327,9 +327,15 @@ def main() -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=list(CONFIGS), default="caustic")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scale", type=int, default=1,
+                    help="divide the resolution by s and the photon count by s^2 (small profiling cases only)")
     a = ap.parse_args()
     a.warmup = max(3, a.warmup)
-    cfg = CONFIGS[a.config]
+    cfg = dict(CONFIGS[a.config])
+    if a.scale > 1:
+        cfg.update(width=cfg["width"] // a.scale, height=cfg["height"] // a.scale,
+                   photons=max(1, cfg["photons"] // (a.scale * a.scale)),
+                   desc=cfg["desc"] + f" (scaled 1/{a.scale} for profiling; not a bench value)")
     if a.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return 0

@@ -9,6 +9,11 @@
 // the order a sequential run of emit_photons.cl produces — and the compaction is fused into the
 // hash kernel.  A path stores at most one photon per bounce, so max_bounces slots per path
 // always suffice, exactly like the reference's photons*max_bounces buffer (renderer.cpp:40).
+//
+// Two forms produce identical results: k_emit (one thread per path) and k_emit_persistent, where
+// each lane runs one path as a state machine (one ray query per step) and the warp refills lanes
+// whose path ended with new paths (__ballot_sync / __popc, one atomicAdd per refill), so short
+// paths (escapes, Russian roulette) do not leave lanes idle while long ones bounce.
 #include "dev_shading.cuh"
 #include "kernels.hpp"
 
@@ -79,21 +84,111 @@ __global__ void __launch_bounds__(128) k_emit(LaunchCtx lc, EmitOut out) {
         atomicAdd(lc.overflow, ovf);
 }
 
+// ---- state machine with lane refill -------------------------------------------------------------
+// One photon path per lane, one ray query per step (emit_photons.cl:49-113 split at
+// scene_intersect); a lane whose path ends is refilled with the next path of the queue.
+struct PhotonPath {
+    const SceneDesc *sc;
+    u32 gid, n_out, depth;
+    u64 slot;
+    Rng rng;
+    float4 origin, dir, power, throughput;
+    IorStack ior;
+};
+
+PHX_DI void pp_start(PhotonPath &p, const SceneDesc *sc, u32 seed, u32 tid, u32 gid) {
+    p.sc = sc;
+    p.gid = gid;
+    p.n_out = 0;
+    p.depth = 0;
+    p.slot = sc->slot_base + tid;
+    p.rng = pcg_seed(seed + tid);
+    sample_light(&p.rng, *sc, &p.origin, &p.dir, &p.power);
+    init_ior_stack(&p.ior, AIR_IOR);
+    p.throughput = f4(1.0f, 1.0f, 1.0f, 0.0f);
+}
+
+// Consumes the pending query; returns true while the path continues.
+PHX_DI bool pp_advance(PhotonPath &p, bool hit, const Hit &h, const EmitOut &out) {
+    const SceneDesc &sc = *p.sc;
+    if (!hit)
+        return false;
+    SurfaceHit sh = process_hit(sc, h, p.origin, p.dir);
+    const phx_material mat = sc.materials[sh.mat_index];
+    float cur = current_ior(&p.ior);
+    if (cur != AIR_IOR && mat.thickness > EPS && mat.att_dist > EPS) {
+        float4 vol = beer_lambert(f4(mat.att_color), mat.att_dist, sh.t);
+        p.power *= vol;
+        p.throughput *= vol;
+    }
+    float4 tangent, bitangent;
+    hit_frame(sc, h, sh, &tangent, &bitangent);
+    ShadingContext ctx = evaluate_material(sc, mat, sh.mat_index, sh.uvx, sh.uvy, sh.normal, tangent, bitangent);
+    if (p.depth >= RR_MIN_PHOTON_DEPTH) {
+        float q = fmaxf(p.throughput.x, fmaxf(p.throughput.y, p.throughput.z));
+        q = clampf(q, RR_MIN_Q, RR_MAX_Q);
+        if (random_float(&p.rng) > q)
+            return false;
+        float inv_q = 1.0f / q;
+        p.throughput *= inv_q;
+        p.power *= inv_q;
+    }
+    float4 view = -p.dir;
+    BsdfSample bs = sample_bsdf(&p.rng, ctx, ctx.shading_normal, sh.normal, view, &p.ior, sh.front_face);
+    if (bs.event == BSDF_DIFFUSE && dot(p.dir, sh.normal) < 0.0f) {
+        out.slot_pos[p.slot] = sh.position;
+        out.slot_pd[p.slot] = make_uint2(encode_rgbe(p.power), encode_oct(p.dir));
+        p.slot += sc.n_emit;
+        p.n_out++;
+    }
+    p.power *= bs.throughput;
+    p.throughput *= bs.throughput;
+    float4 side = (dot(bs.dir, sh.normal) > 0.0f) ? sh.normal : -sh.normal;
+    p.origin = sh.position + bs.dir * EPS + side * EPS;
+    p.dir = bs.dir;
+    p.depth++;
+    return p.depth < sc.max_bounces;
+}
+
 __global__ void __launch_bounds__(128) k_emit_persistent(LaunchCtx lc, EmitOut out, u32 *queue) {
     const u32 lane = threadIdx.x & 31u;
+    const u32 lt_mask = (1u << lane) - 1u;
     u32 ovf = 0;
+    PhotonPath p;
+    bool active = false, exhausted = false;
     for (;;) {
-        u32 base = 0;
-        if (lane == 0)
-            base = atomicAdd(queue, 32u);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= lc.total_emit)
+        const u32 need = __ballot_sync(0xffffffffu, !active && !exhausted);
+        if (need) {
+            const u32 leader = __ffs(need) - 1;
+            u32 base = 0;
+            if (lane == leader)
+                base = atomicAdd(queue, (u32)__popc(need));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (!active && !exhausted) {
+                const u32 gid = base + __popc(need & lt_mask);
+                if (gid < lc.total_emit) {
+                    const u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.emit_bases, lc.n_scenes, gid);
+                    const SceneDesc *sc = lc.scenes + s;
+                    pp_start(p, sc, __ldg(&lc.seeds[s]), gid - sc->emit_base, gid);
+                    active = true;
+                    if (sc->max_bounces == 0) {
+                        out.counts[gid] = 0;
+                        active = false;
+                    }
+                } else {
+                    exhausted = true;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, active))
             break;
-        u32 gid = base + lane;
-        if (gid < lc.total_emit) {
-            u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.emit_bases, lc.n_scenes, gid);
-            const SceneDesc &sc = lc.scenes[s];
-            out.counts[gid] = emit_path(sc, __ldg(&lc.seeds[s]), gid - sc.emit_base, out, &ovf);
+        if (active) {
+            Hit h;
+            const bool hit = intersect(*p.sc, p.origin, p.dir, EPS, INF, &h, &ovf);
+            if (!pp_advance(p, hit, h, out)) {
+                out.counts[p.gid] = p.n_out;
+                active = false;
+            }
         }
     }
     if (ovf)

@@ -1,16 +1,38 @@
 // k_trace.cu — camera paths to the first diffuse hit with explicit direct lighting
 // (kernels/trace_rays.cl:14-169), for every pixel of every scene of an engine.
 //
-// Two launch forms share one per-pixel body:
-//  * one thread per pixel;
-//  * persistent warps that drain a global pixel queue 32 pixels at a time.
-// Pixel i of a scene uses pcg_seed(round_seed + i) exactly like the reference, so the result is
-// independent of which lane or block traces it.
+// Two forms produce identical results:
+//  * k_trace: one thread per pixel, the reference's nested loops as written.  A warp then runs
+//    the traversal from several call sites (camera ray, diffuse-NEE shadow ray, specular-NEE
+//    shadow ray, shadow continuation) one after another, and every lane waits for the longest
+//    path of its warp.
+//  * k_trace_persistent: each lane runs its pixel as a state machine that issues ONE ray query
+//    per step (camera ray or shadow ray), so all lanes of a warp traverse together from a single
+//    call site; when a lane's path ends, the warp refills its free lanes with new pixels in one
+//    shot (__ballot_sync / __popc over the free mask, one atomicAdd per refill).  The state
+//    machine replays the reference's statements in the same order with the same RNG draws, only
+//    split at the ray queries.
+// Pixel i of a scene uses pcg_seed(round_seed + i), so results do not depend on which lane or
+// block traces it.
 #include "dev_shading.cuh"
 #include "kernels.hpp"
 
 namespace phx {
 
+struct TraceResult {
+    float4 position, normal, throughput, base_color, direct, emission;
+};
+
+PHX_DI void write_result(const TraceOut &out, u32 gpix, const TraceResult &r) {
+    out.emission[gpix] = r.emission;
+    out.pos[gpix] = r.position;
+    out.normal[gpix] = r.normal;
+    out.throughput[gpix] = r.throughput;
+    out.base_color[gpix] = r.base_color;
+    out.direct[gpix] = r.direct;
+}
+
+// ---- one thread per pixel ---------------------------------------------------------------------
 PHX_DI void trace_pixel(const SceneDesc &sc, u32 seed, u32 tid, const TraceOut &out, u32 gpix, u32 *overflow) {
     u32 width = sc.width, height = sc.height;
     u32 px = tid % width;
@@ -84,12 +106,8 @@ PHX_DI void trace_pixel(const SceneDesc &sc, u32 seed, u32 tid, const TraceOut &
         origin = sh.position + bs.dir * EPS + side * EPS;
         dir = bs.dir;
     }
-    out.emission[gpix] = emission;
-    out.pos[gpix] = position;
-    out.normal[gpix] = normal;
-    out.throughput[gpix] = throughput;
-    out.base_color[gpix] = base_color;
-    out.direct[gpix] = direct;
+    TraceResult r{position, normal, throughput, base_color, direct, emission};
+    write_result(out, gpix, r);
 }
 
 __global__ void __launch_bounds__(128) k_trace(LaunchCtx lc, TraceOut out) {
@@ -104,22 +122,278 @@ __global__ void __launch_bounds__(128) k_trace(LaunchCtx lc, TraceOut out) {
         atomicAdd(lc.overflow, ovf);
 }
 
-// Persistent form: warps pull pixel indices from *queue until it is drained.
+// ---- state machine ------------------------------------------------------------------------------
+enum : u32 { PH_CAMERA = 0, PH_SHADOW = 1 };
+enum : u32 { NEE_DIFFUSE = 0, NEE_SPECULAR = 1, NEE_NONE = 2 };
+
+struct CameraPath {
+    const SceneDesc *sc;
+    u32 gpix;
+    Rng rng;
+    u32 phase, nee_kind, nee_i, depth;
+    float4 origin, dir;         // current query ray
+    float t_min, t_max;
+    float4 throughput, emission;
+    IorStack ior;
+    // shading state kept across the NEE loop (trace_rays.cl:99-147)
+    float4 pos, sn, gn, base, view, f0, bs_dir, bs_thr, nee_sum;
+    float occl, rough;
+    // pending shadow query (shadow_transmittance, light_sampling.h:302-333)
+    float4 m, trans;
+    u32 sh_depth;
+};
+
+PHX_DI void cp_finish(CameraPath &p, const TraceOut &out, bool diffuse_hit) {
+    TraceResult r;
+    r.throughput = p.throughput;
+    if (diffuse_hit) {
+        r.emission = f4(p.emission.x, p.emission.y, p.emission.z, 1.0f);
+        r.position = p.pos;
+        r.normal = p.gn;
+        r.base_color = p.base;
+        r.direct = p.throughput * p.occl * (p.nee_sum / (float)p.sc->direct_samples);
+    } else {
+        r.emission = p.emission;
+        r.position = zero4();
+        r.normal = zero4();
+        r.base_color = zero4();
+        r.direct = zero4();
+    }
+    write_result(out, p.gpix, r);
+}
+
+PHX_DI void cp_start(CameraPath &p, const SceneDesc *sc, u32 seed, u32 tid, u32 gpix) {
+    p.sc = sc;
+    p.gpix = gpix;
+    p.rng = pcg_seed(seed + tid);
+    make_ray(sc->camera, tid % sc->width, tid / sc->width, sc->width, sc->height, &p.rng, &p.origin, &p.dir);
+    p.throughput = white4();
+    p.emission = zero4();
+    init_ior_stack(&p.ior, AIR_IOR);
+    p.depth = 0;
+    p.phase = PH_CAMERA;
+    p.t_min = EPS;
+    p.t_max = INF;
+}
+
+// Runs the NEE loop from sample nee_i until a shadow query is needed (returns true with the query
+// in origin/dir/t_min/t_max) or all samples are done (returns false).
+PHX_DI bool cp_next_shadow(CameraPath &p) {
+    const SceneDesc &sc = *p.sc;
+    while (p.nee_i < sc.direct_samples) {
+        if (p.nee_kind == NEE_DIFFUSE) { // direct_lighting_diffuse, light_sampling.h:335-353
+            LightFragment f;
+            if (!sample_light_fragment(&p.rng, sc, p.pos, p.sn, &f)) {
+                p.nee_sum += zero4();
+                p.nee_i++;
+                continue;
+            }
+            p.m = f.radiance * (p.base / PI);
+            p.dir = f.dir;
+            p.t_max = f.dist - EPS;
+        } else { // direct_lighting_specular, light_sampling.h:355-390
+            float ndv = dot(p.view, p.sn);
+            if (ndv < EPS) {
+                p.nee_sum += zero4();
+                p.nee_i++;
+                continue;
+            }
+            LightFragment f;
+            if (!sample_light_fragment(&p.rng, sc, p.pos, p.sn, &f) || f.n_dot_dir < EPS) {
+                p.nee_sum += zero4();
+                p.nee_i++;
+                continue;
+            }
+            float alpha = p.rough * p.rough;
+            float4 h = normalize(f.dir + p.view);
+            float ndh = fmaxf(dot(p.sn, h), 0.0f);
+            float g = ggx_ndf(ndh, alpha);
+            float4 fr = fresnel4(p.f0, p.view, h);
+            float sm = smith_g1_ggx(f.n_dot_dir, alpha) * smith_g1_ggx(ndv, alpha);
+            float4 spec = f.radiance * g * fr * sm / (4.0f * f.n_dot_dir * ndv);
+            if (dot(spec, spec) < EPS * EPS) {
+                p.nee_sum += zero4();
+                p.nee_i++;
+                continue;
+            }
+            p.m = spec;
+            p.dir = f.dir;
+            p.t_max = f.dist - EPS;
+        }
+        p.origin = p.pos;
+        p.t_min = EPS;
+        p.trans = white4();
+        p.sh_depth = 0;
+        p.phase = PH_SHADOW;
+        return true;
+    }
+    return false;
+}
+
+// Continues the camera path after its BSDF sample (trace_rays.cl:149-160).  Returns true when a
+// new camera query is pending, false when the path has ended (outputs written).
+PHX_DI bool cp_continue(CameraPath &p, const TraceOut &out) {
+    p.throughput *= p.bs_thr;
+    if (p.depth >= RR_MIN_RAY_DEPTH) {
+        float q = fmaxf(p.throughput.x, fmaxf(p.throughput.y, p.throughput.z));
+        q = clampf(q, RR_MIN_Q, RR_MAX_Q);
+        if (random_float(&p.rng) > q) {
+            cp_finish(p, out, false);
+            return false;
+        }
+        p.throughput *= 1.0f / q;
+    }
+    float4 side = (dot(p.bs_dir, p.gn) > 0.0f) ? p.gn : -p.gn;
+    p.origin = p.pos + p.bs_dir * EPS + side * EPS;
+    p.dir = p.bs_dir;
+    p.depth++;
+    if (p.depth >= MAX_RAY_BOUNCES) {
+        cp_finish(p, out, false);
+        return false;
+    }
+    p.phase = PH_CAMERA;
+    p.t_min = EPS;
+    p.t_max = INF;
+    return true;
+}
+
+// After the NEE loop of a bounce: finish (diffuse) or continue (specular events).
+PHX_DI bool cp_after_nee(CameraPath &p, const TraceOut &out) {
+    if (p.nee_kind == NEE_DIFFUSE) {
+        cp_finish(p, out, true);
+        return false;
+    }
+    if (p.nee_kind == NEE_SPECULAR)
+        p.emission += p.throughput * (p.nee_sum / (float)p.sc->direct_samples);
+    return cp_continue(p, out);
+}
+
+// Consumes the result of the pending query; returns true while the path needs another query.
+PHX_DI bool cp_advance(CameraPath &p, bool hit, const Hit &h, const TraceOut &out) {
+    const SceneDesc &sc = *p.sc;
+    if (p.phase == PH_SHADOW) {
+        bool done_ray = false;
+        float4 contrib;
+        if (!hit) {
+            contrib = p.trans;
+            done_ray = true;
+        } else {
+            u32 mi = tri_mat(sc, h.tri);
+            const phx_material &mat = sc.materials[mi];
+            if (mat.transmission < EPS) {
+                contrib = zero4();
+                done_ray = true;
+            } else {
+                float4 base = f4(mat.base_color);
+                if (mat.diff_index != NO_TEXTURE) {
+                    SurfaceHit s = process_hit(sc, h, p.origin, p.dir);
+                    base *= srgb_to_linear(sample_texture_uv(sc, mi, mat.diff_index, s.uvx, s.uvy, 0));
+                }
+                if (mat.att_dist > EPS)
+                    p.trans *= beer_lambert(f4(mat.att_color), mat.att_dist, h.t - p.t_min);
+                p.trans *= base * mat.transmission;
+                if (dot(p.trans, p.trans) < EPS) {
+                    contrib = zero4();
+                    done_ray = true;
+                } else {
+                    p.t_min = h.t + EPS;
+                    p.sh_depth++;
+                    if (p.sh_depth >= MAX_RAY_BOUNCES) {
+                        contrib = p.trans;
+                        done_ray = true;
+                    }
+                }
+            }
+        }
+        if (!done_ray)
+            return true; // next transmittance query along the same shadow ray
+        p.nee_sum += p.m * contrib;
+        p.nee_i++;
+        if (cp_next_shadow(p))
+            return true;
+        return cp_after_nee(p, out);
+    }
+    // camera query (trace_rays.cl:64-147)
+    if (!hit) {
+        if (sc.has_env)
+            p.emission += p.throughput * sample_envmap(sc, p.dir);
+        cp_finish(p, out, false);
+        return false;
+    }
+    SurfaceHit sh = process_hit(sc, h, p.origin, p.dir);
+    const phx_material mat = sc.materials[sh.mat_index];
+    float cur = current_ior(&p.ior);
+    if (cur != AIR_IOR && mat.thickness > EPS && mat.att_dist > EPS)
+        p.throughput *= beer_lambert(f4(mat.att_color), mat.att_dist, sh.t);
+    float4 tangent, bitangent;
+    hit_frame(sc, h, sh, &tangent, &bitangent);
+    ShadingContext ctx = evaluate_material(sc, mat, sh.mat_index, sh.uvx, sh.uvy, sh.normal, tangent, bitangent);
+    p.emission += p.throughput * ctx.emissive;
+    p.view = -p.dir;
+    BsdfSample bs = sample_bsdf(&p.rng, ctx, ctx.shading_normal, sh.normal, p.view, &p.ior, sh.front_face);
+    p.pos = sh.position;
+    p.sn = ctx.shading_normal;
+    p.gn = sh.normal;
+    p.base = ctx.base_color;
+    p.occl = ctx.occlusion;
+    p.rough = ctx.roughness;
+    p.bs_dir = bs.dir;
+    p.bs_thr = bs.throughput;
+    p.nee_sum = zero4();
+    p.nee_i = 0;
+    if (bs.event == BSDF_DIFFUSE) {
+        p.nee_kind = NEE_DIFFUSE;
+    } else if (bs.event == BSDF_METALLIC) {
+        p.nee_kind = NEE_SPECULAR;
+        p.f0 = ctx.base_color;
+    } else if (bs.event == BSDF_FRESNEL) {
+        float ratio = (cur - ctx.ior) / (cur + ctx.ior);
+        float r0 = ratio * ratio;
+        p.nee_kind = NEE_SPECULAR;
+        p.f0 = f4(r0, r0, r0, 0.0f);
+    } else {
+        p.nee_kind = NEE_NONE;
+        return cp_continue(p, out);
+    }
+    if (cp_next_shadow(p))
+        return true;
+    return cp_after_nee(p, out);
+}
+
 __global__ void __launch_bounds__(128) k_trace_persistent(LaunchCtx lc, TraceOut out, u32 *queue) {
     const u32 lane = threadIdx.x & 31u;
+    const u32 lt_mask = (1u << lane) - 1u;
     u32 ovf = 0;
+    CameraPath p;
+    bool active = false, exhausted = false;
     for (;;) {
-        u32 base = 0;
-        if (lane == 0)
-            base = atomicAdd(queue, 32u);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= lc.total_pixels)
+        // refill free lanes with new pixels: one atomic per warp
+        const u32 need = __ballot_sync(0xffffffffu, !active && !exhausted);
+        if (need) {
+            const u32 leader = __ffs(need) - 1;
+            u32 base = 0;
+            if (lane == leader)
+                base = atomicAdd(queue, (u32)__popc(need));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (!active && !exhausted) {
+                const u32 gid = base + __popc(need & lt_mask);
+                if (gid < lc.total_pixels) {
+                    const u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gid);
+                    const SceneDesc *sc = lc.scenes + s;
+                    cp_start(p, sc, __ldg(&lc.seeds[s]), gid - sc->pixel_base, gid);
+                    active = true;
+                } else {
+                    exhausted = true;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, active))
             break;
-        u32 gid = base + lane;
-        if (gid < lc.total_pixels) {
-            u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gid);
-            const SceneDesc &sc = lc.scenes[s];
-            trace_pixel(sc, __ldg(&lc.seeds[s]), gid - sc.pixel_base, out, gid, &ovf);
+        if (active) {
+            Hit h;
+            const bool any = p.phase == PH_SHADOW && p.sc->any_transmissive == 0;
+            const bool hit = intersect(*p.sc, p.origin, p.dir, p.t_min, p.t_max, &h, &ovf, any);
+            active = cp_advance(p, hit, h, out);
         }
     }
     if (ovf)

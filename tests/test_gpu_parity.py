@@ -221,6 +221,24 @@ def test_rounds_end_to_end(name):
     assert np.allclose(img.reshape(-1, 3), oimg, atol=1e-6)
 
 
+@pytest.mark.parametrize("name", list(SCENES))
+def test_persistent_and_simple_kernels_agree(name):
+    """The lane-refill state-machine kernels and the one-thread-per-item kernels are bit-identical."""
+    scene, args = make(name)
+    with P.Renderer(args) as a, P.Renderer(args) as b:
+        a.set_scene(scene)
+        b.set_scene(scene)
+        t = b.tuning()
+        assert t.persistent == 1
+        t.persistent = 0
+        b.set_tuning(t)
+        a.iterate(2)
+        b.iterate(2)
+        for buf in ["HP_POS", "HP_DIRECT", "HP_EMISSION", "EMIT_COUNT", "PHOTON_POS", "PHOTON_POWER", "FLUX",
+                    "RADIANCE"]:
+            assert np.array_equal(a.read(buf).view(np.uint32), b.read(buf).view(np.uint32)), buf
+
+
 def test_graph_replay_equals_plain_rounds():
     scene, args = make("caustic")
     with P.Renderer(args) as a, P.Renderer(args) as b:
