@@ -206,6 +206,10 @@ def run_ours(a, cfg: dict) -> dict | None:
     scene = P.SceneData.generate(cfg["kind"], seed=1, width=args.width, height=args.height, detail=cfg["detail"])
     r = P.Renderer(args, device=local)
     r.set_scene(scene)
+    if a.simple:
+        t = r.tuning()
+        t.persistent = 0
+        r.set_tuning(t)
     ext = torch.cuda.ExternalStream(r.stream(), device=local)
     r.iterate(max(3, a.warmup))
 
@@ -327,6 +331,7 @@ def main() -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=list(CONFIGS), default="caustic")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--simple", action="store_true", help="one-thread-per-item kernels instead of lane refill")
     ap.add_argument("--scale", type=int, default=1,
                     help="divide the resolution by s and the photon count by s^2 (small profiling cases only)")
     a = ap.parse_args()

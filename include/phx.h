@@ -154,12 +154,14 @@ typedef struct phx_params {
     uint32_t direct_samples;       /* --direct-samples (1..128) */
     uint32_t seed;                 /* --seed */
     uint32_t flags;                /* PHX_F_* */
-    uint32_t reserved[7];
+    uint32_t bvh_leaf_size;        /* max triangles per leaf of the traversal tree (0 = 4) */
+    uint32_t reserved[6];
 } phx_params;
 
 /* flags */
 #define PHX_F_DEFAULT 0u
 #define PHX_F_SIMPLE_TRAVERSAL 1u /* one-thread-per-ray kernels instead of the persistent ones */
+#define PHX_F_REFERENCE_BVH 2u    /* traverse the reference's median-split tree instead of the SAH tree */
 
 /* Counters and sizes of a context. */
 typedef struct phx_info {
@@ -179,7 +181,9 @@ typedef struct phx_info {
     phx_photon_hash_data hash;
     uint32_t kernels_per_round;   /* CUDA kernels one round launches (all scenes of an engine) */
     uint32_t sort_passes;         /* counting-sort digit passes per round */
-    uint32_t reserved[6];
+    uint32_t trav_depth;          /* depth of the device traversal tree */
+    uint32_t trav_inner_nodes;    /* inner (child-pair) nodes of the device traversal tree */
+    uint32_t reserved[4];
 } phx_info;
 
 /* Buffers readable / writable through phx_read_buffer / phx_write_buffer, always in the

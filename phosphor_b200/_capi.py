@@ -24,7 +24,7 @@ STATUS_NAMES = {0: "PHX_OK", 1: "PHX_E_INVALID", 2: "PHX_E_OOM", 3: "PHX_E_CUDA"
 PHX_NO_TEXTURE = 0xFFFFFFFF
 PHX_LIGHT_POINT, PHX_LIGHT_SPOT, PHX_LIGHT_DIRECTIONAL, PHX_LIGHT_TEXTURED = range(4)
 PHX_SCENE_CORNELL, PHX_SCENE_CAUSTIC, PHX_SCENE_ATRIUM = range(3)
-PHX_F_DEFAULT, PHX_F_SIMPLE_TRAVERSAL = 0, 1
+PHX_F_DEFAULT, PHX_F_SIMPLE_TRAVERSAL, PHX_F_REFERENCE_BVH = 0, 1, 2
 
 BUFFERS = ["HP_POS", "HP_NORMAL", "HP_THROUGHPUT", "HP_BASE_COLOR", "HP_DIRECT", "HP_EMISSION", "FLUX",
            "PHOTON_WEIGHT", "RADIANCE", "PHOTON_POS", "PHOTON_POWER", "PHOTON_DIR", "PHOTON_HASH", "CELL_COUNT",
@@ -110,7 +110,7 @@ class Params(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("photons_per_round", C.c_uint32),
                 ("max_photon_bounces", C.c_uint32), ("grid_res", C.c_uint32), ("sppm_alpha", C.c_float),
                 ("direct_samples", C.c_uint32), ("seed", C.c_uint32), ("flags", C.c_uint32),
-                ("reserved", C.c_uint32 * 7)]
+                ("bvh_leaf_size", C.c_uint32), ("reserved", C.c_uint32 * 6)]
 
 
 class Info(C.Structure):
@@ -118,7 +118,8 @@ class Info(C.Structure):
                                           "bucket_count", "n_photons", "n_bvh_nodes", "bvh_depth", "rounds_done")] + \
                [("total_photons_emitted", C.c_uint64), ("stack_overflows", C.c_uint32), ("error_flags", C.c_uint32),
                 ("_pad0", C.c_uint32 * 2), ("hash", PhotonHashData), ("kernels_per_round", C.c_uint32),
-                ("sort_passes", C.c_uint32), ("reserved", C.c_uint32 * 6)]
+                ("sort_passes", C.c_uint32), ("trav_depth", C.c_uint32), ("trav_inner_nodes", C.c_uint32),
+                ("reserved", C.c_uint32 * 4)]
 
 
 class SceneSpec(C.Structure):

@@ -89,12 +89,16 @@ struct Hit {
 };
 
 constexpr int TRAV_STACK = 64;
+constexpr u32 LEAF_FIRST_BITS = 27; // leaf reference: ~(first | (count-1) << 27)
 
 // Möller–Trumbore test of hit.h:45-78 with the reference's dot(float4) including w terms.
-// ow, dw: w components of the ray origin and direction (always +-0 in practice).
+// ow, dw: w components of the ray origin and direction (always +-0 in practice).  The record's
+// w lanes carry the material index (r0.w) and the reference leaf rank (r1.w); the test itself
+// uses the reference's zero w components of the edge vectors.
 PHX_DI bool tri_test(const float4 *rec, float ox, float oy, float oz, float ow, float dx, float dy, float dz, float dw,
-                     float t_min, float t_max, float *tt, float *tu, float *tv) {
+                     float t_min, float t_max, float *tt, float *tu, float *tv, u32 *rank) {
     float4 r0 = __ldg(rec + 0), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2);
+    *rank = __float_as_uint(r1.w);
     // e1 = r1.xyz, e2 = r2.xyz (precomputed v1-v0, v2-v0 with the same float subtraction)
     float hx = dy * r2.z - dz * r2.y;
     float hy = dz * r2.x - dx * r2.z;
@@ -122,15 +126,18 @@ PHX_DI bool tri_test(const float4 *rec, float ox, float oy, float oz, float ow, 
     return true;
 }
 
-PHX_DI void box2(const float4 &a, const float4 &b, const float4 &c, float ix, float iy, float iz, float ox, float oy,
-                 float oz, float t_min, float t_max, float *tl, float *tr, bool *hl, bool *hr) {
+// Slab test of both children of a node.  Box tests only decide what is skipped, never which
+// triangle is hit (boxes are expanded by 1e-3, far above rounding), so they use fused
+// multiply-add t = box*inv - origin*inv: one instruction per plane.
+PHX_DI void box2(const float4 &a, const float4 &b, const float4 &c, float ix, float iy, float iz, float oix, float oiy,
+                 float oiz, float t_min, float t_max, float *tl, float *tr, bool *hl, bool *hr) {
     // left child: a = (minx, maxx, miny, maxy), c.xy = (minz, maxz); right: b, c.zw
-    float lx0 = (a.x - ox) * ix, lx1 = (a.y - ox) * ix;
-    float ly0 = (a.z - oy) * iy, ly1 = (a.w - oy) * iy;
-    float lz0 = (c.x - oz) * iz, lz1 = (c.y - oz) * iz;
-    float rx0 = (b.x - ox) * ix, rx1 = (b.y - ox) * ix;
-    float ry0 = (b.z - oy) * iy, ry1 = (b.w - oy) * iy;
-    float rz0 = (c.z - oz) * iz, rz1 = (c.w - oz) * iz;
+    float lx0 = __fmaf_rn(a.x, ix, -oix), lx1 = __fmaf_rn(a.y, ix, -oix);
+    float ly0 = __fmaf_rn(a.z, iy, -oiy), ly1 = __fmaf_rn(a.w, iy, -oiy);
+    float lz0 = __fmaf_rn(c.x, iz, -oiz), lz1 = __fmaf_rn(c.y, iz, -oiz);
+    float rx0 = __fmaf_rn(b.x, ix, -oix), rx1 = __fmaf_rn(b.y, ix, -oix);
+    float ry0 = __fmaf_rn(b.z, iy, -oiy), ry1 = __fmaf_rn(b.w, iy, -oiy);
+    float rz0 = __fmaf_rn(c.z, iz, -oiz), rz1 = __fmaf_rn(c.w, iz, -oiz);
     float lnear = fmaxf(fmaxf(fminf(lx0, lx1), fminf(ly0, ly1)), fmaxf(fminf(lz0, lz1), t_min));
     float lfar = fminf(fminf(fmaxf(lx0, lx1), fmaxf(ly0, ly1)), fminf(fmaxf(lz0, lz1), t_max));
     float rnear = fmaxf(fmaxf(fminf(rx0, rx1), fminf(ry0, ry1)), fmaxf(fminf(rz0, rz1), t_min));
@@ -145,9 +152,10 @@ PHX_DI void box2(const float4 &a, const float4 &b, const float4 &c, float ix, fl
 // `any` stops at the first accepted hit (only valid where the caller needs no specific hit).
 PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, float t_max, Hit *hit, u32 *overflow,
                       bool any = false) {
-    float ix = 1.0f / d.x, iy = 1.0f / d.y, iz = 1.0f / d.z;
+    const float ix = 1.0f / d.x, iy = 1.0f / d.y, iz = 1.0f / d.z;
+    const float oix = o.x * ix, oiy = o.y * iy, oiz = o.z * iz;
     float closest = t_max;
-    i32 best = -1;
+    i32 best = -1, best_rank = -1;
     float bu = 0.0f, bv = 0.0f;
     i32 stack_ref[TRAV_STACK];
     float stack_t[TRAV_STACK];
@@ -160,7 +168,7 @@ PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, floa
             int4 ch = __ldg(reinterpret_cast<const int4 *>(cn + 3));
             float tl, tr;
             bool hl, hr;
-            box2(a, b, c, ix, iy, iz, o.x, o.y, o.z, t_min, closest, &tl, &tr, &hl, &hr);
+            box2(a, b, c, ix, iy, iz, oix, oiy, oiz, t_min, closest, &tl, &tr, &hl, &hr);
             if (hl && hr) {
                 i32 nearr = ch.x, farr = ch.y;
                 float tfar = tr;
@@ -187,20 +195,32 @@ PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, floa
             }
         }
         if (node != 0x7fffffff) {
-            // leaf
-            i32 rank = ~node;
-            float t, u, v;
-            if (tri_test(sc.trirec + 3 * (size_t)rank, o.x, o.y, o.z, o.w, d.x, d.y, d.z, d.w, t_min, closest, &t, &u,
-                         &v)) {
-                if (t < closest || rank > best) {
-                    closest = t;
-                    best = rank;
-                    bu = u;
-                    bv = v;
-                    if (any)
-                        break;
+            // leaf: triangles [first, first + count)
+            const u32 enc = (u32)~node;
+            const u32 first = enc & ((1u << LEAF_FIRST_BITS) - 1u);
+            const u32 count = (enc >> LEAF_FIRST_BITS) + 1u;
+            bool stop = false;
+            for (u32 k = 0; k < count; k++) {
+                float t, u, v;
+                u32 rank;
+                if (tri_test(sc.trirec + 3 * (size_t)(first + k), o.x, o.y, o.z, o.w, d.x, d.y, d.z, d.w, t_min,
+                             closest, &t, &u, &v, &rank)) {
+                    // t <= closest here; at equal t the reference keeps the larger leaf rank
+                    if (t < closest || (i32)rank > best_rank) {
+                        closest = t;
+                        best = (i32)(first + k);
+                        best_rank = (i32)rank;
+                        bu = u;
+                        bv = v;
+                        if (any) {
+                            stop = true;
+                            break;
+                        }
+                    }
                 }
             }
+            if (stop)
+                break;
         }
         // pop the next entry that can still hold a hit
         bool found = false;

@@ -140,8 +140,20 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
     }
     if (!bvh_build(s.triangles, s.n_triangles, S.nodes, &S.depth))
         return fail(PHX_E_INVALID, "degenerate or infinite triangle bounding box (bounding_box.h:17-28)");
+    // Traversal tree: binned SAH over the same expanded boxes (fewer node visits), or the
+    // reference tree itself.  Either returns the reference's hit for every ray: the closest t,
+    // ties broken by the reference leaf rank carried in each triangle record.
     PackedBvh pk;
-    bvh_pack(S.nodes, s.triangles, pk);
+    bool sah = !(p.flags & PHX_F_REFERENCE_BVH);
+    if (sah) {
+        std::vector<uint32_t> ranks = reference_leaf_ranks(S.nodes, s.n_triangles);
+        sah = bvh_build_sah(s.triangles, s.n_triangles, ranks, p.bvh_leaf_size ? p.bvh_leaf_size : 4u, pk) &&
+              pk.depth + 2 < (uint32_t)TRAV_STACK;
+    }
+    if (!sah)
+        bvh_pack(S.nodes, s.triangles, pk);
+    S.trav_depth = sah ? pk.depth : S.depth;
+    S.trav_inner = (uint32_t)(pk.cnodes.size() / 16);
     const uint32_t n = s.n_triangles;
     S.n_tris = n;
     std::vector<float> nrm((size_t)n * 12), tan((size_t)n * 12), uv((size_t)n * 8);
@@ -906,6 +918,8 @@ int Engine::info(uint32_t s, phx_info *o) {
     o->total_photons_emitted = S.total_emitted;
     o->hash = S.hash;
     o->sort_passes = radix_passes(key_bits);
+    o->trav_depth = S.trav_depth;
+    o->trav_inner_nodes = S.trav_inner;
     // seeds, trace, emit, count scan, compaction, hash, cell scan, 3 per sort pass, records, gather
     o->kernels_per_round = 9 + 3 * o->sort_passes;
     CK(cudaStreamSynchronize(st));

@@ -31,8 +31,9 @@ struct DevBuf {
 struct SceneSlot {
     phx_params prm{};
     phx_photon_hash_data hash{};
-    std::vector<phx_bvh_node> nodes;
+    std::vector<phx_bvh_node> nodes; // the reference tree (read-back, grid box, tie-break ranks)
     uint32_t depth = 0;
+    uint32_t trav_depth = 0, trav_inner = 0; // the device traversal tree
     uint32_t n_tris = 0;
     std::vector<DevBuf> bufs;
     SceneDesc desc{};

@@ -166,6 +166,42 @@ bool bvh_build(const phx_triangle *tris, uint32_t n, std::vector<phx_bvh_node> &
     return true;
 }
 
+namespace {
+
+// 48-byte triangle record: {v0 | material bits}, {v1-v0 | reference rank bits}, {v2-v0 | 0}.  The
+// edge vectors use the same float subtraction as hit.h:48-49, so the device test is bit-identical.
+void put_trirec(float *r, const phx_triangle &tr, uint32_t ref_rank) {
+    r[0] = tr.v0.x; r[1] = tr.v0.y; r[2] = tr.v0.z; r[3] = u2f(tr.mat_index);
+    r[4] = tr.v1.x - tr.v0.x; r[5] = tr.v1.y - tr.v0.y; r[6] = tr.v1.z - tr.v0.z; r[7] = u2f(ref_rank);
+    r[8] = tr.v2.x - tr.v0.x; r[9] = tr.v2.y - tr.v0.y; r[10] = tr.v2.z - tr.v0.z; r[11] = 0.0f;
+}
+
+// leaf reference: ~(first | (count-1) << 27)
+constexpr uint32_t LEAF_FIRST_BITS = 27;
+int32_t leaf_ref(uint32_t first, uint32_t count) { return ~(int32_t)(first | ((count - 1u) << LEAF_FIRST_BITS)); }
+
+void put_pair(float *c, const float lo0[3], const float hi0[3], const float lo1[3], const float hi1[3], int32_t r0,
+              int32_t r1) {
+    c[0] = lo0[0]; c[1] = hi0[0]; c[2] = lo0[1]; c[3] = hi0[1];
+    c[4] = lo1[0]; c[5] = hi1[0]; c[6] = lo1[1]; c[7] = hi1[1];
+    c[8] = lo0[2]; c[9] = hi0[2]; c[10] = lo1[2]; c[11] = hi1[2];
+    int32_t refs[2] = {r0, r1};
+    std::memcpy(&c[12], refs, 8);
+}
+
+} // namespace
+
+std::vector<uint32_t> reference_leaf_ranks(const std::vector<phx_bvh_node> &nodes, uint32_t n_tris) {
+    std::vector<uint32_t> rank(n_tris, 0);
+    uint32_t k = 0;
+    for (const auto &nd : nodes) { // pre-order = the reference's left-first visiting order of leaves
+        uint32_t t = f2u(nd.min.w);
+        if (t != 0xFFFFFFFFu && t < n_tris)
+            rank[t] = k++;
+    }
+    return rank;
+}
+
 void bvh_pack(const std::vector<phx_bvh_node> &nodes, const phx_triangle *tris, PackedBvh &out) {
     const size_t nn = nodes.size();
     std::vector<int32_t> ref(nn);
@@ -174,35 +210,205 @@ void bvh_pack(const std::vector<phx_bvh_node> &nodes, const phx_triangle *tris, 
         if (f2u(nodes[i].min.w) == 0xFFFFFFFFu)
             ref[i] = (int32_t)n_inner++;
         else
-            ref[i] = ~(int32_t)n_leaf++;
+            ref[i] = leaf_ref(n_leaf++, 1);
     }
     out.cnodes.assign((size_t)n_inner * 16, 0.0f);
     out.trirec.assign((size_t)n_leaf * 12, 0.0f);
     out.leaf_tri.assign(n_leaf, 0);
     out.root = ref[0];
+    out.max_leaf = 1;
     for (size_t i = 0; i < nn; i++) {
         const phx_bvh_node &nd = nodes[i];
         if (ref[i] >= 0) {
             const phx_bvh_node &L = nodes[i + 1];
             uint32_t ri = f2u(nd.max.w);
             const phx_bvh_node &R = nodes[ri];
-            float *c = &out.cnodes[(size_t)ref[i] * 16];
-            c[0] = L.min.x; c[1] = L.max.x; c[2] = L.min.y; c[3] = L.max.y;
-            c[4] = R.min.x; c[5] = R.max.x; c[6] = R.min.y; c[7] = R.max.y;
-            c[8] = L.min.z; c[9] = L.max.z; c[10] = R.min.z; c[11] = R.max.z;
-            int32_t refs[2] = {ref[i + 1], ref[ri]};
-            std::memcpy(&c[12], refs, 8);
+            const float lo0[3] = {L.min.x, L.min.y, L.min.z}, hi0[3] = {L.max.x, L.max.y, L.max.z};
+            const float lo1[3] = {R.min.x, R.min.y, R.min.z}, hi1[3] = {R.max.x, R.max.y, R.max.z};
+            put_pair(&out.cnodes[(size_t)ref[i] * 16], lo0, hi0, lo1, hi1, ref[i + 1], ref[ri]);
         } else {
-            uint32_t rank = (uint32_t)~ref[i];
+            uint32_t rank = (uint32_t)(~ref[i]) & ((1u << LEAF_FIRST_BITS) - 1u);
             uint32_t t = f2u(nd.min.w);
             out.leaf_tri[rank] = t;
-            const phx_triangle &tr = tris[t];
-            float *r = &out.trirec[(size_t)rank * 12];
-            r[0] = tr.v0.x; r[1] = tr.v0.y; r[2] = tr.v0.z; r[3] = u2f(tr.mat_index);
-            r[4] = tr.v1.x - tr.v0.x; r[5] = tr.v1.y - tr.v0.y; r[6] = tr.v1.z - tr.v0.z; r[7] = 0.0f;
-            r[8] = tr.v2.x - tr.v0.x; r[9] = tr.v2.y - tr.v0.y; r[10] = tr.v2.z - tr.v0.z; r[11] = 0.0f;
+            put_trirec(&out.trirec[(size_t)rank * 12], tris[t], rank);
         }
     }
+}
+
+// Binned SAH (surface area heuristic, MacDonald & Booth 1990; binning after Wald 2007): 32 bins
+// per axis over the primitive centroids, cost = 1 + (A_l N_l + A_r N_r) / A, leaf cost = N.
+bool bvh_build_sah(const phx_triangle *tris, uint32_t n, const std::vector<uint32_t> &ref_rank, uint32_t max_leaf,
+                   PackedBvh &out) {
+    if (!tris || n == 0 || n >= (1u << LEAF_FIRST_BITS))
+        return false;
+    max_leaf = std::max(1u, std::min(max_leaf, 16u));
+    struct Prim {
+        float lo[3], hi[3], c[3];
+        uint32_t tri;
+    };
+    std::vector<Prim> P(n);
+    for (uint32_t i = 0; i < n; i++) {
+        Box b;
+        if (!triangle_box(tris[i], b))
+            return false;
+        for (int a = 0; a < 3; a++) {
+            P[i].lo[a] = b.lo[a];
+            P[i].hi[a] = b.hi[a];
+            P[i].c[a] = 0.5f * (b.lo[a] + b.hi[a]);
+        }
+        P[i].tri = i;
+    }
+    auto area = [](const float *l, const float *h) {
+        float x = h[0] - l[0], y = h[1] - l[1], z = h[2] - l[2];
+        return x * y + y * z + z * x;
+    };
+    constexpr int NB = 32;
+    out.cnodes.clear();
+    out.cnodes.reserve((size_t)n * 16);
+    out.trirec.assign((size_t)n * 12, 0.0f);
+    out.leaf_tri.assign(n, 0);
+    out.max_leaf = max_leaf;
+    uint32_t next_tri = 0, depth = 0;
+    int32_t root = 0;
+    // work item: primitive range [b, e) at depth d whose reference goes to child `side` of `node`
+    // (node == ~0u: the root).  Indices, not pointers: cnodes grows while building.
+    struct Frame {
+        uint32_t b, e, d;
+        uint32_t node;
+        int side;
+    };
+    std::vector<Frame> work{{0, n, 0, 0xFFFFFFFFu, 0}};
+    while (!work.empty()) {
+        Frame f = work.back();
+        work.pop_back();
+        const Frame &pd = f;
+        const uint32_t b = f.b, e = f.e, cnt = e - b;
+        depth = std::max(depth, f.d);
+        float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
+        float clo[3] = {1e30f, 1e30f, 1e30f}, chi[3] = {-1e30f, -1e30f, -1e30f};
+        for (uint32_t i = b; i < e; i++)
+            for (int a = 0; a < 3; a++) {
+                lo[a] = std::min(lo[a], P[i].lo[a]);
+                hi[a] = std::max(hi[a], P[i].hi[a]);
+                clo[a] = std::min(clo[a], P[i].c[a]);
+                chi[a] = std::max(chi[a], P[i].c[a]);
+            }
+        int32_t ref;
+        // choose a split
+        float best = 1e30f;
+        int bax = -1, bbin = 0;
+        if (cnt > 1) {
+            for (int a = 0; a < 3; a++) {
+                float ext = chi[a] - clo[a];
+                if (!(ext > 0.0f))
+                    continue;
+                int bc[NB] = {0};
+                float bl[NB][3], bh[NB][3];
+                for (int k = 0; k < NB; k++)
+                    for (int j = 0; j < 3; j++) {
+                        bl[k][j] = 1e30f;
+                        bh[k][j] = -1e30f;
+                    }
+                const float sc = NB / ext;
+                for (uint32_t i = b; i < e; i++) {
+                    int k = std::min(NB - 1, (int)((P[i].c[a] - clo[a]) * sc));
+                    bc[k]++;
+                    for (int j = 0; j < 3; j++) {
+                        bl[k][j] = std::min(bl[k][j], P[i].lo[j]);
+                        bh[k][j] = std::max(bh[k][j], P[i].hi[j]);
+                    }
+                }
+                float ra[NB];
+                int rn[NB];
+                float rl[3] = {1e30f, 1e30f, 1e30f}, rh[3] = {-1e30f, -1e30f, -1e30f};
+                int acc = 0;
+                for (int k = NB - 1; k > 0; k--) {
+                    acc += bc[k];
+                    for (int j = 0; j < 3; j++) {
+                        rl[j] = std::min(rl[j], bl[k][j]);
+                        rh[j] = std::max(rh[j], bh[k][j]);
+                    }
+                    rn[k] = acc;
+                    ra[k] = acc ? area(rl, rh) : 0.0f;
+                }
+                float ll[3] = {1e30f, 1e30f, 1e30f}, lh[3] = {-1e30f, -1e30f, -1e30f};
+                int ln = 0;
+                for (int k = 1; k < NB; k++) {
+                    ln += bc[k - 1];
+                    for (int j = 0; j < 3; j++) {
+                        ll[j] = std::min(ll[j], bl[k - 1][j]);
+                        lh[j] = std::max(lh[j], bh[k - 1][j]);
+                    }
+                    if (ln == 0 || rn[k] == 0)
+                        continue;
+                    float c = ln * area(ll, lh) + rn[k] * ra[k];
+                    if (c < best) {
+                        best = c;
+                        bax = a;
+                        bbin = k;
+                    }
+                }
+            }
+        }
+        const float parea = area(lo, hi);
+        const bool make_leaf = cnt == 1 || (cnt <= max_leaf && (bax < 0 || 1.0f + best / parea >= (float)cnt));
+        if (make_leaf && cnt <= max_leaf) {
+            uint32_t first = next_tri;
+            // keep triangles of a leaf in reference-rank order (irrelevant for results, stable)
+            std::sort(P.begin() + b, P.begin() + e,
+                      [&](const Prim &x, const Prim &y) { return ref_rank[x.tri] < ref_rank[y.tri]; });
+            for (uint32_t i = b; i < e; i++) {
+                out.leaf_tri[next_tri] = P[i].tri;
+                put_trirec(&out.trirec[(size_t)next_tri * 12], tris[P[i].tri], ref_rank[P[i].tri]);
+                next_tri++;
+            }
+            ref = leaf_ref(first, cnt);
+            if (pd.node == 0xFFFFFFFFu)
+                root = ref;
+            else
+                std::memcpy(&out.cnodes[(size_t)pd.node * 16 + 12 + pd.side], &ref, 4);
+            continue;
+        }
+        uint32_t mid;
+        if (bax >= 0) {
+            const float ext = chi[bax] - clo[bax], sc = NB / ext;
+            auto it = std::partition(P.begin() + b, P.begin() + e, [&](const Prim &p) {
+                return std::min(NB - 1, (int)((p.c[bax] - clo[bax]) * sc)) < bbin;
+            });
+            mid = (uint32_t)(it - P.begin());
+            if (mid == b || mid == e)
+                mid = b + cnt / 2;
+        } else { // all centroids coincide: object median
+            mid = b + cnt / 2;
+        }
+        uint32_t node = (uint32_t)(out.cnodes.size() / 16);
+        out.cnodes.resize(out.cnodes.size() + 16, 0.0f);
+        ref = (int32_t)node;
+        if (pd.node == 0xFFFFFFFFu)
+            root = ref;
+        else
+            std::memcpy(&out.cnodes[(size_t)pd.node * 16 + 12 + pd.side], &ref, 4);
+        // child boxes
+        float l0[3] = {1e30f, 1e30f, 1e30f}, h0[3] = {-1e30f, -1e30f, -1e30f};
+        float l1[3] = {1e30f, 1e30f, 1e30f}, h1[3] = {-1e30f, -1e30f, -1e30f};
+        for (uint32_t i = b; i < mid; i++)
+            for (int a = 0; a < 3; a++) {
+                l0[a] = std::min(l0[a], P[i].lo[a]);
+                h0[a] = std::max(h0[a], P[i].hi[a]);
+            }
+        for (uint32_t i = mid; i < e; i++)
+            for (int a = 0; a < 3; a++) {
+                l1[a] = std::min(l1[a], P[i].lo[a]);
+                h1[a] = std::max(h1[a], P[i].hi[a]);
+            }
+        put_pair(&out.cnodes[(size_t)node * 16], l0, h0, l1, h1, 0, 0);
+        // depth-first: left child processed next (pre-order layout)
+        work.push_back({mid, e, f.d + 1, node, 1});
+        work.push_back({b, mid, f.d + 1, node, 0});
+    }
+    out.root = root;
+    out.depth = depth;
+    return next_tri == n;
 }
 
 // build_photon_hash_info (photon_hash.h:41-50)

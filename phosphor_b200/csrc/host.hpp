@@ -14,14 +14,24 @@ namespace phx {
 // (bounding_box.h:17-28 traps there).
 bool bvh_build(const phx_triangle *tris, uint32_t n, std::vector<phx_bvh_node> &nodes, uint32_t *depth);
 
-// Device packing of a reference-layout BVH (see dev_scene.cuh).
+// Device packing of a traversal BVH (see dev_scene.cuh).
 struct PackedBvh {
-    std::vector<float> cnodes;     // 16 floats per inner node
-    std::vector<float> trirec;     // 12 floats per triangle, leaf order
-    std::vector<uint32_t> leaf_tri; // leaf rank -> original triangle index
+    std::vector<float> cnodes;      // 16 floats per inner node (child pair)
+    std::vector<float> trirec;      // 12 floats per triangle, device (leaf) order
+    std::vector<uint32_t> leaf_tri; // device triangle index -> original triangle index
     int32_t root = 0;
+    uint32_t max_leaf = 1;
+    uint32_t depth = 0;
 };
+// Leaf rank of every triangle in the reference tree (pre-order over leaves): the tie-break key of
+// hits at exactly equal t (hit.h:68 keeps the last tested one).
+std::vector<uint32_t> reference_leaf_ranks(const std::vector<phx_bvh_node> &nodes, uint32_t n_tris);
+// The reference tree itself re-packed as child pairs (one triangle per leaf).
 void bvh_pack(const std::vector<phx_bvh_node> &nodes, const phx_triangle *tris, PackedBvh &out);
+// A binned-SAH tree over the same expanded triangle boxes (bounding_box.h:48-61), leaves of up to
+// max_leaf triangles; triangle records carry the reference leaf rank for tie-breaking.
+bool bvh_build_sah(const phx_triangle *tris, uint32_t n, const std::vector<uint32_t> &ref_rank, uint32_t max_leaf,
+                   PackedBvh &out);
 
 phx_photon_hash_data hash_info(const phx_bvh_node &root, uint32_t grid_res);
 void scene_sphere(const phx_bvh_node &root, phx_f4 *center, float *radius);

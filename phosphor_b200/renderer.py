@@ -41,6 +41,9 @@ class ArgsList:
     direct_samples: int = 16
     output_dir: str = ""
     save_snapshots: bool = False
+    # B200 build knobs (no reference counterpart; results do not depend on them)
+    flags: int = 0           # PHX_F_*
+    bvh_leaf_size: int = 0   # 0 = library default
 
     def params(self) -> A.Params:
         p = A.Params()
@@ -51,7 +54,8 @@ class ArgsList:
         p.sppm_alpha = self.sppm_alpha
         p.direct_samples = self.direct_samples
         p.seed = self.seed
-        p.flags = 0
+        p.flags = self.flags
+        p.bvh_leaf_size = self.bvh_leaf_size
         return p
 
 
