@@ -46,7 +46,7 @@ CONFIGS = {
                    desc="procedural atrium, 262,898 triangles, 1920x1080, 2^22 photons/iter, depth 16"),
 }
 METRIC = "Mphotons/s"
-ALGO_STAGES = ["trace", "emit", "emit_scan", "hash", "cell_scan", "sort", "records", "gather"]
+ALGO_STAGES = ["trace", "shadow", "emit", "emit_scan", "hash", "cell_scan", "sort", "records", "gather"]
 
 
 def load_peaks() -> tuple[float, str]:
@@ -172,10 +172,11 @@ def run_reference(a, cfg: dict) -> dict:
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
-def algorithmic_bytes(stage: str, P: int, Ne: int, Ns: int, C: int, scene_bytes: int) -> int:
+def algorithmic_bytes(stage: str, P: int, Ne: int, Ns: int, C: int, scene_bytes: int, ds: int = 16) -> int:
     """Compulsory bytes per round of each stage (roofline table)."""
     return {
-        "trace": 96 * P + scene_bytes,
+        "trace": 96 * P + 32 * P * ds + scene_bytes,
+        "shadow": 48 * P * ds + 48 * P + scene_bytes,
         "emit": 24 * Ns + scene_bytes,
         "emit_scan": 8 * Ne + 48 * Ns,
         "hash": 16 * Ns + 4 * Ns + 4 * C + 8 * Ns,

@@ -310,7 +310,8 @@ typedef struct phx_tuning {
     uint32_t trace_blocks_per_sm;  /* persistent grid: resident blocks per SM */
     uint32_t emit_blocks_per_sm;
     uint32_t persistent;        /* 1 = persistent lane-refill kernels, 0 = one thread per item */
-    uint32_t reserved[6];
+    uint32_t nee_wavefront;     /* 1 = diffuse-hit NEE shadow rays traced by a separate wavefront */
+    uint32_t reserved[5];
 } phx_tuning;
 PHX_API int phx_get_tuning(void *ctx, phx_tuning *out);
 PHX_API int phx_set_tuning(void *ctx, const phx_tuning *in);
@@ -320,7 +321,8 @@ PHX_API int phx_set_tuning(void *ctx, const phx_tuning *in);
  * per-stage averages; enabling or disabling drops the captured graph. */
 PHX_API int phx_profile(void *ctx, int enable);
 /* Average milliseconds per round of each stage since phx_profile(ctx, 1), in the order
- * seeds, trace, emit, emit scan + compaction, hash, cell scan, sort, records, gather (n >= 9). */
+ * seeds, trace, shadow (NEE wavefront + resolve), emit, emit scan + compaction, hash, cell scan,
+ * sort, records, gather (n >= 10). */
 PHX_API int phx_stage_ms(void *ctx, float *out, uint32_t n);
 /* The CUDA stream (cudaStream_t) every stage of the context or batch is enqueued on. */
 PHX_API uint64_t phx_get_stream(void *ctx);

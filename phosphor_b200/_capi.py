@@ -40,7 +40,7 @@ BUF_DTYPE.update({name: (np.uint32, 1) for name in ["PHOTON_POWER", "PHOTON_DIR"
 BUF_DTYPE["PHOTON_WEIGHT"] = (np.float32, 1)
 BUF_DTYPE["BVH_NODES"] = (np.float32, 8)
 
-STAGES = ["seeds", "trace", "emit", "emit_scan", "hash", "cell_scan", "sort", "records", "gather"]
+STAGES = ["seeds", "trace", "shadow", "emit", "emit_scan", "hash", "cell_scan", "sort", "records", "gather"]
 
 
 class f4(C.Structure):
@@ -129,7 +129,8 @@ class SceneSpec(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("trace_block", "emit_block", "gather_block", "trace_blocks_per_sm",
-                                          "emit_blocks_per_sm", "persistent")] + [("reserved", C.c_uint32 * 6)]
+                                          "emit_blocks_per_sm", "persistent", "nee_wavefront")] + \
+               [("reserved", C.c_uint32 * 5)]
 
 
 SIZES = {Triangle: 176, Material: 96, UvTransformBlock: 192, Light: 128, CameraParams: 112, BvhNode: 32,

@@ -66,7 +66,8 @@ struct __align__(16) SceneDesc {
     u64 slot_base;        // first photon slot of this scene (slot j of path t at slot_base + j*n_emit + t)
     u32 flags;
     u32 any_transmissive; // 0 -> shadow rays can stop at the first hit
-    u32 pad1[2];
+    u32 nee_base;         // first deferred-NEE sample slot of this scene (pixel i, sample d at nee_base + i*ds + d)
+    u32 pad1;
 };
 
 // scene of global index gid: bases[s] <= gid < bases[s+1] (n+1 prefix offsets)

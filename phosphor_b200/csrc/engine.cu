@@ -58,7 +58,8 @@ Engine::~Engine() {
     for (auto &s : sc)
         for (auto &b : s.bufs)
             b.release();
-    DevBuf *all[] = {&d_desc, &d_pix_bases, &d_emit_bases, &d_seeds, &d_rng, &d_err, &d_ovf, &d_queue, &d_ntotal,
+    DevBuf *all[] = {&d_desc, &d_pix_bases, &d_emit_bases, &d_nee_bases, &nee_ray, &nee_val, &d_seeds, &d_rng,
+                     &d_err, &d_ovf, &d_queue, &d_ntotal,
                      &flux, &weight, &radiance, &slot_pos, &slot_pd, &counts, &offsets, &ph_pos, &ph_pd, &keys,
                      &cell_count, &cell_start, &sk0, &sk1, &sv0, &sv1, &s_posdir, &s_power, &scan_scr, &radix_scr,
                      &img_rgb, &img_ldr};
@@ -264,6 +265,10 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
     d.emit_base = *emit;
     d.cell_base = *cell;
     d.slot_base = *slot;
+    d.nee_base = total_nee;
+    if ((uint64_t)total_nee + (uint64_t)d.n_pixels * d.direct_samples > 0x7fffffffull)
+        return fail(PHX_E_INVALID, "too many direct-lighting samples per round for 31-bit slot indices");
+    total_nee += d.n_pixels * d.direct_samples;
     d.flags = p.flags;
     d.any_transmissive = 0;
     for (uint32_t m = 0; m < s.n_materials; m++)
@@ -312,18 +317,22 @@ int Engine::create(const phx_scene *scenes, const phx_params *params, uint32_t n
         key_bits++;
 
     std::vector<SceneDesc> descs(n);
-    std::vector<uint32_t> pb(n + 1), eb(n + 1), rng(n);
+    std::vector<uint32_t> pb(n + 1), eb(n + 1), nb(n + 1), rng(n);
     for (uint32_t i = 0; i < n; i++) {
         descs[i] = sc[i].desc;
         pb[i] = sc[i].desc.pixel_base;
         eb[i] = sc[i].desc.emit_base;
+        nb[i] = sc[i].desc.nee_base;
         rng[i] = pcg_seed(sc[i].prm.seed).state; // renderer.cpp:54
     }
     pb[n] = total_pixels;
     eb[n] = total_emit;
+    nb[n] = total_nee;
     int r;
     if ((r = upload(d_desc, descs.data(), sizeof(SceneDesc) * n)) || (r = upload(d_pix_bases, pb.data(), 4 * pb.size())) ||
-        (r = upload(d_emit_bases, eb.data(), 4 * eb.size())) || (r = upload(d_rng, rng.data(), 4 * n)) ||
+        (r = upload(d_emit_bases, eb.data(), 4 * eb.size())) || (r = upload(d_nee_bases, nb.data(), 4 * nb.size())) ||
+        (r = nee_ray.alloc(16 * (size_t)total_nee)) || (r = nee_val.alloc(16 * (size_t)total_nee)) ||
+        (r = upload(d_rng, rng.data(), 4 * n)) ||
         (r = upload(d_seeds, nullptr, 4 * n)) || (r = upload(d_err, nullptr, 16)) || (r = upload(d_ovf, nullptr, 16)) ||
         (r = upload(d_queue, nullptr, 16)) || (r = upload(d_ntotal, nullptr, 16)))
         return r;
@@ -349,7 +358,8 @@ int Engine::create(const phx_scene *scenes, const phx_params *params, uint32_t n
     tune.gather_block = 128;
     tune.trace_blocks_per_sm = 8;
     tune.emit_blocks_per_sm = 8;
-    tune.persistent = 1;
+    tune.persistent = 0;
+    tune.nee_wavefront = 1;
     for (uint32_t i = 0; i < n; i++)
         if (params[i].flags & PHX_F_SIMPLE_TRAVERSAL)
             tune.persistent = 0;
@@ -368,6 +378,9 @@ LaunchCtx Engine::lc() const {
     l.seeds = d_seeds.as<u32>();
     l.err = d_err.as<u32>();
     l.overflow = d_ovf.as<u32>();
+    l.nee_bases = d_nee_bases.as<u32>();
+    l.total_nee = total_nee;
+    l.nee_defer = tune.nee_wavefront ? 1u : 0u;
     return l;
 }
 
@@ -404,11 +417,16 @@ void Engine::enq_seeds() {
 
 void Engine::enq_trace() {
     ev(ST_TRACE, false);
-    TraceOut o{hp[0].as<float4>(), hp[1].as<float4>(), hp[2].as<float4>(),
-               hp[3].as<float4>(), hp[4].as<float4>(), hp[5].as<float4>()};
-    launch_trace(lc(), o, (int)tune.trace_block, (int)tune.persistent, (int)tune.trace_blocks_per_sm, d_queue.as<u32>(),
+    TraceOut o{hp[0].as<float4>(), hp[1].as<float4>(), hp[2].as<float4>(), hp[3].as<float4>(),
+               hp[4].as<float4>(), hp[5].as<float4>(), nee_ray.as<float4>(), nee_val.as<float4>()};
+    const LaunchCtx l = lc();
+    launch_trace(l, o, (int)tune.trace_block, (int)tune.persistent, (int)tune.trace_blocks_per_sm, d_queue.as<u32>(),
                  st);
     ev(ST_TRACE, true);
+    ev(ST_SHADOW, false);
+    launch_shadow(l, o, (int)tune.trace_block, st);
+    launch_nee_resolve(l, o, st);
+    ev(ST_SHADOW, true);
     stage_state |= 1;
 }
 
@@ -920,8 +938,9 @@ int Engine::info(uint32_t s, phx_info *o) {
     o->sort_passes = radix_passes(key_bits);
     o->trav_depth = S.trav_depth;
     o->trav_inner_nodes = S.trav_inner;
-    // seeds, trace, emit, count scan, compaction, hash, cell scan, 3 per sort pass, records, gather
-    o->kernels_per_round = 9 + 3 * o->sort_passes;
+    // seeds, trace, [shadow, resolve], emit, count scan, compaction, hash, cell scan, 3 per sort
+    // pass, records, gather
+    o->kernels_per_round = 9 + 3 * o->sort_passes + (tune.nee_wavefront ? 2 : 0);
     CK(cudaStreamSynchronize(st));
     uint32_t v[2] = {0, 0};
     CK(cudaMemcpy(&v[0], d_ovf.p, 4, cudaMemcpyDeviceToHost));

@@ -42,7 +42,19 @@ struct SceneSlot {
     uint32_t n_photons_last = 0;
 };
 
-enum Stage { ST_SEEDS = 0, ST_TRACE, ST_EMIT, ST_EMIT_SCAN, ST_HASH, ST_CELL_SCAN, ST_SORT, ST_RECORDS, ST_GATHER, ST__N };
+enum Stage {
+    ST_SEEDS = 0,
+    ST_TRACE,
+    ST_SHADOW,
+    ST_EMIT,
+    ST_EMIT_SCAN,
+    ST_HASH,
+    ST_CELL_SCAN,
+    ST_SORT,
+    ST_RECORDS,
+    ST_GATHER,
+    ST__N
+};
 
 class Engine {
   public:
@@ -77,7 +89,7 @@ class Engine {
     int device = 0;
     cudaStream_t st = nullptr;
     std::vector<SceneSlot> sc;
-    uint32_t total_pixels = 0, total_emit = 0, total_cells = 0;
+    uint32_t total_pixels = 0, total_emit = 0, total_cells = 0, total_nee = 0;
     uint64_t total_slots = 0, max_photons = 0;
     uint32_t key_bits = 1;
     phx_tuning tune{};
@@ -92,7 +104,8 @@ class Engine {
     void ev(int stage, bool end);
     void accumulate_profile();
 
-    DevBuf d_desc, d_pix_bases, d_emit_bases, d_seeds, d_rng, d_err, d_ovf, d_queue, d_ntotal;
+    DevBuf d_desc, d_pix_bases, d_emit_bases, d_nee_bases, d_seeds, d_rng, d_err, d_ovf, d_queue, d_ntotal;
+    DevBuf nee_ray, nee_val;
     DevBuf hp[6], flux, weight, radiance;
     DevBuf slot_pos, slot_pd, counts, offsets, ph_pos, ph_pd, keys, cell_count, cell_start;
     DevBuf sk0, sk1, sv0, sv1, s_posdir, s_power, scan_scr, radix_scr, img_rgb, img_ldr;

@@ -32,8 +32,27 @@ PHX_DI void write_result(const TraceOut &out, u32 gpix, const TraceResult &r) {
     out.direct[gpix] = r.direct;
 }
 
+// Deferred diffuse-hit NEE (trace_rays.cl:103-118).  The reference's path ends after this loop
+// and its RNG draws (light choice, light point) never depend on the shadow rays' outcome, so the
+// loop is split: here the samples are drawn in order and each shadow ray is recorded; the shadow
+// wavefront traces them; the resolve kernel sums the contributions in sample order.
+PHX_DI void record_nee(const SceneDesc &sc, Rng *rng, float4 pos, float4 sn, float4 base, const TraceOut &out,
+                       u32 slot) {
+    for (u32 d = 0; d < sc.direct_samples; d++, slot++) {
+        LightFragment f;
+        if (sample_light_fragment(rng, sc, pos, sn, &f)) { // direct_lighting_diffuse, light_sampling.h:345-352
+            out.nee_ray[slot] = f4(f.dir.x, f.dir.y, f.dir.z, f.dist);
+            out.nee_val[slot] = f.radiance * (base / PI);
+        } else {
+            out.nee_ray[slot] = f4(0.0f, 0.0f, 0.0f, -1.0f); // returns BLACK
+            out.nee_val[slot] = zero4();
+        }
+    }
+}
+
 // ---- one thread per pixel ---------------------------------------------------------------------
-PHX_DI void trace_pixel(const SceneDesc &sc, u32 seed, u32 tid, const TraceOut &out, u32 gpix, u32 *overflow) {
+PHX_DI void trace_pixel(const SceneDesc &sc, u32 seed, u32 tid, const TraceOut &out, u32 gpix, u32 *overflow,
+                        bool defer) {
     u32 width = sc.width, height = sc.height;
     u32 px = tid % width;
     u32 py = tid / width;
@@ -67,14 +86,21 @@ PHX_DI void trace_pixel(const SceneDesc &sc, u32 seed, u32 tid, const TraceOut &
         float4 view = -dir;
         BsdfSample bs = sample_bsdf(&rng, ctx, ctx.shading_normal, sh.normal, view, &ior, sh.front_face);
         if (bs.event == BSDF_DIFFUSE) {
-            float4 sum = zero4();
-            for (u32 d = 0; d < sc.direct_samples; d++)
-                sum += direct_lighting_diffuse(&rng, sc, sh.position, ctx.shading_normal, ctx.base_color, overflow);
+            if (defer) {
+                record_nee(sc, &rng, sh.position, ctx.shading_normal, ctx.base_color, out,
+                           sc.nee_base + tid * sc.direct_samples);
+                direct = f4(ctx.occlusion, 0.0f, 0.0f, 0.0f); // the resolve kernel completes it
+            } else {
+                float4 sum = zero4();
+                for (u32 d = 0; d < sc.direct_samples; d++)
+                    sum += direct_lighting_diffuse(&rng, sc, sh.position, ctx.shading_normal, ctx.base_color,
+                                                   overflow);
+                direct = throughput * ctx.occlusion * (sum / (float)sc.direct_samples);
+            }
             emission = f4(emission.x, emission.y, emission.z, 1.0f);
             position = sh.position;
             normal = sh.normal;
             base_color = ctx.base_color;
-            direct = throughput * ctx.occlusion * (sum / (float)sc.direct_samples);
             break;
         }
         if (bs.event == BSDF_METALLIC) {
@@ -117,7 +143,7 @@ __global__ void __launch_bounds__(128) k_trace(LaunchCtx lc, TraceOut out) {
     u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gid);
     const SceneDesc &sc = lc.scenes[s];
     u32 ovf = 0;
-    trace_pixel(sc, __ldg(&lc.seeds[s]), gid - sc.pixel_base, out, gid, &ovf);
+    trace_pixel(sc, __ldg(&lc.seeds[s]), gid - sc.pixel_base, out, gid, &ovf, lc.nee_defer != 0);
     if (ovf)
         atomicAdd(lc.overflow, ovf);
 }
@@ -128,7 +154,7 @@ enum : u32 { NEE_DIFFUSE = 0, NEE_SPECULAR = 1, NEE_NONE = 2 };
 
 struct CameraPath {
     const SceneDesc *sc;
-    u32 gpix;
+    u32 gpix, tid;
     Rng rng;
     u32 phase, nee_kind, nee_i, depth;
     float4 origin, dir;         // current query ray
@@ -143,7 +169,7 @@ struct CameraPath {
     u32 sh_depth;
 };
 
-PHX_DI void cp_finish(CameraPath &p, const TraceOut &out, bool diffuse_hit) {
+PHX_DI void cp_finish(CameraPath &p, const TraceOut &out, bool diffuse_hit, bool deferred = false) {
     TraceResult r;
     r.throughput = p.throughput;
     if (diffuse_hit) {
@@ -151,7 +177,8 @@ PHX_DI void cp_finish(CameraPath &p, const TraceOut &out, bool diffuse_hit) {
         r.position = p.pos;
         r.normal = p.gn;
         r.base_color = p.base;
-        r.direct = p.throughput * p.occl * (p.nee_sum / (float)p.sc->direct_samples);
+        r.direct = deferred ? f4(p.occl, 0.0f, 0.0f, 0.0f)
+                            : p.throughput * p.occl * (p.nee_sum / (float)p.sc->direct_samples);
     } else {
         r.emission = p.emission;
         r.position = zero4();
@@ -165,6 +192,7 @@ PHX_DI void cp_finish(CameraPath &p, const TraceOut &out, bool diffuse_hit) {
 PHX_DI void cp_start(CameraPath &p, const SceneDesc *sc, u32 seed, u32 tid, u32 gpix) {
     p.sc = sc;
     p.gpix = gpix;
+    p.tid = tid;
     p.rng = pcg_seed(seed + tid);
     make_ray(sc->camera, tid % sc->width, tid / sc->width, sc->width, sc->height, &p.rng, &p.origin, &p.dir);
     p.throughput = white4();
@@ -269,7 +297,7 @@ PHX_DI bool cp_after_nee(CameraPath &p, const TraceOut &out) {
 }
 
 // Consumes the result of the pending query; returns true while the path needs another query.
-PHX_DI bool cp_advance(CameraPath &p, bool hit, const Hit &h, const TraceOut &out) {
+PHX_DI bool cp_advance(CameraPath &p, bool hit, const Hit &h, const TraceOut &out, bool defer) {
     const SceneDesc &sc = *p.sc;
     if (p.phase == PH_SHADOW) {
         bool done_ray = false;
@@ -343,6 +371,11 @@ PHX_DI bool cp_advance(CameraPath &p, bool hit, const Hit &h, const TraceOut &ou
     p.nee_i = 0;
     if (bs.event == BSDF_DIFFUSE) {
         p.nee_kind = NEE_DIFFUSE;
+        if (defer) {
+            record_nee(sc, &p.rng, p.pos, p.sn, p.base, out, sc.nee_base + p.tid * sc.direct_samples);
+            cp_finish(p, out, true, true);
+            return false;
+        }
     } else if (bs.event == BSDF_METALLIC) {
         p.nee_kind = NEE_SPECULAR;
         p.f0 = ctx.base_color;
@@ -393,11 +426,70 @@ __global__ void __launch_bounds__(128) k_trace_persistent(LaunchCtx lc, TraceOut
             Hit h;
             const bool any = p.phase == PH_SHADOW && p.sc->any_transmissive == 0;
             const bool hit = intersect(*p.sc, p.origin, p.dir, p.t_min, p.t_max, &h, &ovf, any);
-            active = cp_advance(p, hit, h, out);
+            active = cp_advance(p, hit, h, out, lc.nee_defer != 0);
         }
     }
     if (ovf)
         atomicAdd(lc.overflow, ovf);
+}
+
+// ---- shadow wavefront ---------------------------------------------------------------------------
+// One thread per recorded NEE sample; the ds samples of a pixel are consecutive threads, so a warp
+// traces shadow rays from one or two hit points toward the same light: coherent traversal.
+__global__ void __launch_bounds__(128) k_shadow(LaunchCtx lc, TraceOut out) {
+    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= lc.total_nee)
+        return;
+    const u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.nee_bases, lc.n_scenes, g);
+    const SceneDesc &sc = lc.scenes[s];
+    const u32 pixel = (g - sc.nee_base) / sc.direct_samples;
+    const u32 gpix = sc.pixel_base + pixel;
+    if (out.emission[gpix].w != 1.0f)
+        return; // no diffuse hit point: the slot was not used this round
+    const float4 ray = out.nee_ray[g];
+    float4 contrib;
+    if (ray.w < 0.0f) {
+        contrib = zero4(); // sample_light_fragment failed: direct_lighting_diffuse returned BLACK
+    } else {
+        u32 ovf = 0;
+        const float4 pos = out.pos[gpix];
+        const float4 trans = shadow_transmittance(sc, pos, f4(ray.x, ray.y, ray.z, 0.0f), ray.w, &ovf);
+        contrib = out.nee_val[g] * trans; // frag.radiance * (base / PI) * trans
+        if (ovf)
+            atomicAdd(lc.overflow, ovf);
+    }
+    out.nee_val[g] = contrib;
+}
+
+// Sums each pixel's samples in sample order (trace_rays.cl:104-118).
+__global__ void __launch_bounds__(256) k_nee_resolve(LaunchCtx lc, TraceOut out) {
+    const u32 gpix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gpix >= lc.total_pixels)
+        return;
+    if (out.emission[gpix].w != 1.0f)
+        return;
+    const u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gpix);
+    const SceneDesc &sc = lc.scenes[s];
+    const u32 ds = sc.direct_samples;
+    const float4 *v = out.nee_val + sc.nee_base + (size_t)(gpix - sc.pixel_base) * ds;
+    float4 sum = zero4();
+    for (u32 d = 0; d < ds; d++)
+        sum += v[d];
+    const float occl = out.direct[gpix].x;
+    out.direct[gpix] = out.throughput[gpix] * occl * (sum / (float)ds);
+}
+
+void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int block, cudaStream_t st) {
+    (void)block;
+    if (!lc.nee_defer || lc.total_nee == 0)
+        return;
+    k_shadow<<<(lc.total_nee + 127) / 128, 128, 0, st>>>(lc, out);
+}
+
+void launch_nee_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st) {
+    if (!lc.nee_defer || lc.total_pixels == 0)
+        return;
+    k_nee_resolve<<<(lc.total_pixels + 255) / 256, 256, 0, st>>>(lc, out);
 }
 
 void launch_trace(const LaunchCtx &lc, const TraceOut &out, int block, int persistent, int blocks_per_sm, u32 *queue,

@@ -20,15 +20,24 @@ struct LaunchCtx {
     const u32 *seeds;        // device, one round seed per scene
     u32 *err;                // device error word
     u32 *overflow;           // device traversal-overflow counter
+    const u32 *nee_bases;    // device, n_scenes+1 prefix offsets of deferred-NEE sample slots
+    u32 total_nee;           // sum over scenes of pixels * direct_samples
+    u32 nee_defer;           // 1: diffuse-hit NEE shadow rays go to the shadow wavefront
 };
 
 struct TraceOut {
     float4 *pos, *normal, *throughput, *base_color, *direct, *emission;
+    float4 *nee_ray; // per NEE sample slot: (dir.xyz, light distance), w < 0 = no contribution
+    float4 *nee_val; // per slot: radiance * (base / pi); replaced by the contribution in the shadow pass
 };
 
 // Persistent work queue (lane refill): a device counter the kernel drains.
 void launch_trace(const LaunchCtx &lc, const TraceOut &out, int block, int persistent, int blocks_per_sm,
                   u32 *queue, cudaStream_t st);
+// Deferred diffuse-hit NEE: trace every recorded shadow ray (one thread per sample slot), then sum
+// each pixel's samples in sample order into hp_direct.
+void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int block, cudaStream_t st);
+void launch_nee_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st);
 
 struct EmitOut {
     float4 *slot_pos;

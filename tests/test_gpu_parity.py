@@ -222,21 +222,25 @@ def test_rounds_end_to_end(name):
 
 
 @pytest.mark.parametrize("name", list(SCENES))
-def test_persistent_and_simple_kernels_agree(name):
-    """The lane-refill state-machine kernels and the one-thread-per-item kernels are bit-identical."""
+def test_kernel_forms_agree(name):
+    """One-thread-per-item or lane-refill state-machine kernels, with the diffuse-hit NEE inline or
+    deferred to the shadow wavefront: all four forms give identical bits."""
     scene, args = make(name)
-    with P.Renderer(args) as a, P.Renderer(args) as b:
-        a.set_scene(scene)
-        b.set_scene(scene)
-        t = b.tuning()
-        assert t.persistent == 1
-        t.persistent = 0
-        b.set_tuning(t)
-        a.iterate(2)
-        b.iterate(2)
-        for buf in ["HP_POS", "HP_DIRECT", "HP_EMISSION", "EMIT_COUNT", "PHOTON_POS", "PHOTON_POWER", "FLUX",
-                    "RADIANCE"]:
-            assert np.array_equal(a.read(buf).view(np.uint32), b.read(buf).view(np.uint32)), buf
+    outs = []
+    for persistent in (0, 1):
+        for wavefront in (0, 1):
+            with P.Renderer(args) as r:
+                r.set_scene(scene)
+                t = r.tuning()
+                t.persistent, t.nee_wavefront = persistent, wavefront
+                r.set_tuning(t)
+                r.iterate(2)
+                outs.append({b: r.read(b).view(np.uint32).copy() for b in
+                             ["HP_POS", "HP_DIRECT", "HP_EMISSION", "HP_THROUGHPUT", "EMIT_COUNT", "PHOTON_POS",
+                              "PHOTON_POWER", "FLUX", "RADIANCE"]})
+    for o in outs[1:]:
+        for b in o:
+            assert np.array_equal(o[b], outs[0][b]), b
 
 
 @pytest.mark.parametrize("name", list(SCENES))
