@@ -151,8 +151,14 @@ PHX_DI void box2(const float4 &a, const float4 &b, const float4 &c, float ix, fl
 
 // Closest hit in [t_min, t_max] (scene_intersect, hit.h:135-172).  Returns false on a miss.
 // `any` stops at the first accepted hit (only valid where the caller needs no specific hit).
+//
+// Warp-synchronous single-step loop: the lanes that call intersect together stay in lockstep,
+// each iteration advancing every unfinished lane by exactly one node (an inner child pair or a
+// leaf), so neighbouring rays share every node fetch and the warp never runs one lane's inner
+// loop while the others wait.
 PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, float t_max, Hit *hit, u32 *overflow,
                       bool any = false) {
+    constexpr i32 POP = 0x7fffffff;
     const float ix = 1.0f / d.x, iy = 1.0f / d.y, iz = 1.0f / d.z;
     const float oix = o.x * ix, oiy = o.y * iy, oiz = o.z * iz;
     float closest = t_max;
@@ -162,8 +168,12 @@ PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, floa
     float stack_t[TRAV_STACK];
     int sp = 0;
     i32 node = sc.root;
-    for (;;) {
-        while (node >= 0) {
+    bool done = false;
+    const u32 mask = __activemask();
+    while (__any_sync(mask, !done)) {
+        if (done)
+            continue;
+        if (node >= 0) { // inner node: test both children, descend into the nearer hit one
             const float4 *cn = sc.cnodes + 4 * (size_t)node;
             float4 a = __ldg(cn + 0), b = __ldg(cn + 1), c = __ldg(cn + 2);
             int4 ch = __ldg(reinterpret_cast<const int4 *>(cn + 3));
@@ -186,21 +196,13 @@ PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, floa
                     *overflow += 1;
                 }
                 node = nearr;
-            } else if (hl) {
-                node = ch.x;
-            } else if (hr) {
-                node = ch.y;
             } else {
-                node = 0x7fffffff; // pop marker
-                break;
+                node = hl ? ch.x : (hr ? ch.y : POP);
             }
-        }
-        if (node != 0x7fffffff) {
-            // leaf: triangles [first, first + count)
+        } else { // leaf: triangles [first, first + count)
             const u32 enc = (u32)~node;
             const u32 first = enc & ((1u << LEAF_FIRST_BITS) - 1u);
             const u32 count = (enc >> LEAF_FIRST_BITS) + 1u;
-            bool stop = false;
             for (u32 k = 0; k < count; k++) {
                 float t, u, v;
                 u32 rank;
@@ -213,28 +215,24 @@ PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, floa
                         best_rank = (i32)rank;
                         bu = u;
                         bv = v;
-                        if (any) {
-                            stop = true;
-                            break;
-                        }
+                        if (any)
+                            done = true;
                     }
                 }
             }
-            if (stop)
-                break;
+            node = POP;
         }
-        // pop the next entry that can still hold a hit
-        bool found = false;
-        while (sp > 0) {
-            sp--;
-            if (stack_t[sp] <= closest) {
-                node = stack_ref[sp];
-                found = true;
-                break;
+        if (node == POP && !done) { // pop the next entry that can still hold a hit
+            done = true;
+            while (sp > 0) {
+                sp--;
+                if (stack_t[sp] <= closest) {
+                    node = stack_ref[sp];
+                    done = false;
+                    break;
+                }
             }
         }
-        if (!found)
-            break;
     }
     hit->t = closest;
     hit->u = bu;
