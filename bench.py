@@ -207,9 +207,9 @@ def run_ours(a, cfg: dict) -> dict | None:
     scene = P.SceneData.generate(cfg["kind"], seed=1, width=args.width, height=args.height, detail=cfg["detail"])
     r = P.Renderer(args, device=local)
     r.set_scene(scene)
-    if a.simple:
+    if a.simple or a.persistent:
         t = r.tuning()
-        t.persistent = 0
+        t.persistent = 1 if a.persistent else 0
         r.set_tuning(t)
     ext = torch.cuda.ExternalStream(r.stream(), device=local)
     r.iterate(max(3, a.warmup))
@@ -324,19 +324,104 @@ def run_ours(a, cfg: dict) -> dict | None:
             "gpu_launches": kernels * a.steps, "kernels_per_round": kernels, "clocks": clk.summary()}
 
 
+def run_batch16(a) -> dict:
+    """16 uneven scenes, all advanced per launch from one captured graph, against the
+    plain per-pass form running the scenes one after another."""
+    import torch
+
+    import phosphor_b200 as P
+    from phosphor_b200 import rmse as R
+    specs = R.config3_specs()
+    scenes = [s.scene() for s in specs]
+    photons = sum(s.photons for s in specs)
+    b = P.Batch(scenes, [s.args() for s in specs])
+    ext = torch.cuda.ExternalStream(b.stream())
+    b.iterate(max(3, a.warmup), graph=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        e0.record(ext)
+        b.iterate(a.steps, graph=True)
+        e1.record(ext)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1) / a.steps
+    b.profile(True)
+    b.iterate(a.steps, graph=True)
+    stages = b.stage_ms()
+    b.close()
+    plain = []
+    for s, sc in zip(specs, scenes):
+        r = P.Renderer(s.args())
+        r.set_scene(sc)
+        r.round()
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            r.round()
+        plain.append((time.perf_counter() - t0) / a.steps)
+        r.close()
+    plain_ms = 1e3 * sum(plain)
+    return {"metric": METRIC, "value": round(photons / (ms * 1e-3) / 1e6, 3), "unit": METRIC, "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scenes)",
+            "config": {"workload": "batch16",
+                       "desc": "16 uneven scenes (12..291k triangles, 256^2..1024^2, 2^16..2^21 photons, alpha "
+                               "U[0.6,0.8]) advanced together, one launch per stage, CUDA-graph replay",
+                       "photons_per_round": photons, "triangles": [sc.n_triangles for sc in scenes]},
+            "plain_sequential": {"value": round(photons / (plain_ms * 1e-3) / 1e6, 3), "unit": METRIC,
+                                 "ms_per_round_all_scenes": round(plain_ms, 3),
+                                 "ms_per_scene": [round(1e3 * t, 3) for t in plain]},
+            "speedup_vs_plain": round(plain_ms / ms, 3), "stage_ms": stages, "clocks": clk.summary()}
+
+
+def time_to_rmse(a) -> dict | None:
+    """Rounds to RMSE <= 0.01 against the FP64 oracle fixture, and the wall time of the graph +
+    batched form against the plain per-pass form (scenes one at a time)."""
+    import numpy as np
+
+    from phosphor_b200 import rmse as R
+    fx = ROOT / "tests" / "golden" / "rmse_refs.npz"
+    if not fx.exists():
+        return None
+    z = np.load(fx)
+    specs = R.rmse_batch()
+    refs = [z[f"scene{i}"].astype(np.float64) / 65535.0 for i in range(len(specs))]
+    r_star, curve = R.rounds_to_target(specs, refs, 0.01, max_rounds=4096, check_every=4)
+    ok = [r for r in r_star if r is not None]
+    t_plain = [R.time_plain(s, 40) for s in specs]
+    t_batch = R.time_batched(specs, 200)
+    out = {"target_rmse": 0.01, "reference": f"FP64 oracle, {int(z['rounds'])} rounds, independent seed",
+           "scenes": len(specs), "rounds_to_target": r_star, "final_rmse": [round(x, 5) for x in curve[-1][1]]}
+    if len(ok) == len(specs):
+        tp = sum(r * t for r, t in zip(r_star, t_plain))
+        tb = max(r_star) * t_batch
+        out.update({"plain_s": round(tp, 3), "graph_batched_s": round(tb, 3), "speedup": round(tp / tb, 2),
+                    "plain_ms_per_round": [round(1e3 * t, 3) for t in t_plain],
+                    "batched_ms_per_round": round(1e3 * t_batch, 3)})
+    return out
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=list(CONFIGS), default="caustic")
+    ap.add_argument("--config", choices=list(CONFIGS) + ["batch16"], default="caustic")
+    ap.add_argument("--no-rmse", action="store_true", help="skip the time-to-RMSE study (1 GPU only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--simple", action="store_true", help="one-thread-per-item kernels instead of lane refill")
+    ap.add_argument("--persistent", action="store_true", help="lane-refill state-machine kernels")
     ap.add_argument("--scale", type=int, default=1,
                     help="divide the resolution by s and the photon count by s^2 (small profiling cases only)")
     a = ap.parse_args()
     a.warmup = max(3, a.warmup)
+    if a.config == "batch16":
+        if a.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "batch16 has no reference arm; use --config"
+                              " caustic"}))
+            return 0
+        print(json.dumps(run_batch16(a)))
+        return 0
     cfg = dict(CONFIGS[a.config])
     if a.scale > 1:
         cfg.update(width=cfg["width"] // a.scale, height=cfg["height"] // a.scale,
@@ -349,6 +434,8 @@ def main() -> int:
         return 0
     out = run_ours(a, cfg)
     if out is not None:
+        if not a.no_rmse and out["n_gpus"] == 1 and a.scale == 1:
+            out["time_to_rmse"] = time_to_rmse(a)
         print(json.dumps(out))
     return 0
 

@@ -358,7 +358,7 @@ int Engine::create(const phx_scene *scenes, const phx_params *params, uint32_t n
     tune.gather_block = 128;
     tune.trace_blocks_per_sm = 8;
     tune.emit_blocks_per_sm = 8;
-    tune.persistent = 0;
+    tune.persistent = 1;
     tune.nee_wavefront = 1;
     for (uint32_t i = 0; i < n; i++)
         if (params[i].flags & PHX_F_SIMPLE_TRAVERSAL)

@@ -835,9 +835,9 @@ void atrium(Gen &g, Pcg &rng, int arch_seg, int env_w, int env_h) {
     }
     phx_light sun{};
     sun.kind = PHX_LIGHT_POINT;
-    V3 sun_pos{3.0, 30.0, 5.0};
+    V3 sun_pos{2.0, 14.0, 3.0};
     sun.position = F4(sun_pos);
-    sun.power = {900.0f, 860.0f, 780.0f, 0.0f};
+    sun.power = {200.0f, 190.0f, 170.0f, 0.0f};
     g.s.lights.push_back(sun);
     sky_envmap(g.s, (uint32_t)env_w, (uint32_t)env_h, sun_pos);
 }
