@@ -78,6 +78,28 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
+CLI = PKG / "phx_render"
+HOST_DIR = PKG / "host"
+
+
+def build_cli(force: bool = False, verbose: bool = False) -> Path:
+    """phx_render: the reference's command line over libphx.so (C++ host, C ABI only)."""
+    srcs = [HOST_DIR / "renderer.cpp", HOST_DIR / "main.cpp"]
+    deps = srcs + [HOST_DIR / "renderer.hpp", INCLUDE / "phx.h", LIB]
+    if not force and CLI.exists() and CLI.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
+        return CLI
+    tmp = CLI.with_suffix(".tmp")
+    cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-I", str(INCLUDE), "-o", str(tmp), *map(str, srcs),
+           f"-L{PKG}", "-lphx", "-Wl,-rpath,$ORIGIN", "-lpthread"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"phx_render build failed\n{res.stdout}\n{res.stderr}")
+    os.replace(tmp, CLI)
+    if verbose:
+        print(f"built {CLI}")
+    return CLI
+
+
 def build_oracle(force: bool = False, verbose: bool = False) -> Path:
     """Compiles the CPU oracle (test infrastructure only; see oracle/phx_oracle.hpp)."""
     srcs = [ORACLE_DIR / "oracle_capi.cpp"]
@@ -112,6 +134,7 @@ def main(argv=None) -> int:
     ap.add_argument("--ptxas", action="store_true", help="print register/spill report")
     a = ap.parse_args(argv)
     build_library(a.force, verbose=True)
+    build_cli(a.force, verbose=True)
     build_oracle(a.force, verbose=True)
     if a.ptxas:
         print(ptxas_report())

@@ -39,32 +39,52 @@ PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
     float found = 0.0f;
     const u32 *cs = g.cell_start + sc.cell_base;
     const float denom = 2.0f * r_sq;
-    for (u32 i = 0; i < 27; i++) {
-        i32 cx = (i32)(i % 3) - 1;
-        i32 cy = (i32)((i / 3) % 3) - 1;
-        i32 cz = (i32)((i / 9) % 3) - 1;
-        float px = pos.x, py = pos.y, pz = pos.z;
-        px += (float)cx * grid.cx;
-        py += (float)cy * grid.cy;
-        pz += (float)cz * grid.cz;
-        u32 h = get_hash(px, py, pz, grid);
-        if (h == 0)
+    // The 27 cells x their photons, flattened into one sequence per pixel in the reference's order
+    // (cell i = 0..26, photons in cell order): each iteration of the warp-synchronous loop moves
+    // every lane one step along its own sequence, so lanes with short and long cells stay busy.
+    u32 i = 0, k = 0, end = 0; // current cell index, photon cursor, end of the current cell
+    const u32 mask = __activemask();
+    bool more = true;
+    while (__any_sync(mask, more)) {
+        if (!more)
             continue;
-        u32 start = min(__ldg(&cs[h]), g.n_cap);
-        u32 end = min(__ldg(&cs[h + 1]), g.n_cap);
-        for (u32 k = start; k < end; k++) {
-            float4 p = __ldg(&g.s_posdir[k]);
-            float dx = pos.x - p.x, dy = pos.y - p.y, dz = pos.z - p.z, dw = pos.w - 0.0f;
-            float dsq = ((dx * dx + dy * dy) + dz * dz) + dw * dw;
-            if (dsq >= r_sq)
+        if (k >= end) { // advance to the next non-empty cell (photon_hash.h:65-82)
+            for (;;) {
+                if (i >= 27) {
+                    more = false;
+                    break;
+                }
+                const i32 cx = (i32)(i % 3) - 1;
+                const i32 cy = (i32)((i / 3) % 3) - 1;
+                const i32 cz = (i32)((i / 9) % 3) - 1;
+                float px = pos.x, py = pos.y, pz = pos.z;
+                px += (float)cx * grid.cx;
+                py += (float)cy * grid.cy;
+                pz += (float)cz * grid.cz;
+                const u32 h = get_hash(px, py, pz, grid);
+                i++;
+                if (h == 0)
+                    continue;
+                k = min(__ldg(&cs[h]), g.n_cap);
+                end = min(__ldg(&cs[h + 1]), g.n_cap);
+                if (k < end)
+                    break;
+            }
+            if (!more)
                 continue;
-            float4 pd = decode_oct(__float_as_uint(p.w));
-            if (dot(pd, nrm) > 0.0f)
-                continue;
-            float w = GAUSS_ALPHA * (1.0f - (1.0f - pm_expf((-GAUSS_BETA) * dsq / denom)) / GAUSS_DENOM);
-            nf += w * decode_rgbe(__ldg(&g.s_power[k]));
-            found += w;
         }
+        const float4 p = __ldg(&g.s_posdir[k]);
+        const float dx = pos.x - p.x, dy = pos.y - p.y, dz = pos.z - p.z, dw = pos.w - 0.0f;
+        const float dsq = ((dx * dx + dy * dy) + dz * dz) + dw * dw;
+        if (dsq < r_sq) {
+            const float4 pd = decode_oct(__float_as_uint(p.w));
+            if (!(dot(pd, nrm) > 0.0f)) {
+                const float w = GAUSS_ALPHA * (1.0f - (1.0f - pm_expf((-GAUSS_BETA) * dsq / denom)) / GAUSS_DENOM);
+                nf += w * decode_rgbe(__ldg(&g.s_power[k]));
+                found += w;
+            }
+        }
+        k++;
     }
     if (found > 0.0f) {
         float nw = wso + sc.alpha * found;
