@@ -335,6 +335,27 @@ PHX_API uint64_t phx_get_stream(void *ctx);
  * device-side waits). */
 PHX_API int phx_selftest_lookback_timeout(int device, uint32_t n, uint32_t *err_flags);
 
+/* ---- allocation-free exclusive scan -------------------------------------------------------------
+ * No counterpart in the reference.  out[i] = in[0] + ... + in[i-1] over n uint32 elements (sums
+ * wrap mod 2^32), the same decoupled look-back scan the rounds use for photon offsets and cell
+ * starts, and *total (device pointer, optional) receives the sum of all n.  For callers that may
+ * not allocate device memory: a host whose device memory belongs to a caching or arena allocator
+ * that has reserved the HBM, a plugin held to a fixed memory budget, or a latency-bound loop that
+ * may not pay cudaMalloc/cudaFree's implicit synchronisation after start-up.  The scan's scratch
+ * (tile tickets and look-back status words) is a static device array of 33,024 bytes per device
+ * instead of a caller-provided buffer, so the call allocates nothing; it clears that scratch itself
+ * on every call, so in/out need no initial contents.
+ *   - in, out, total: device pointers on the current device (in and out may not overlap).
+ *   - n <= 16,777,216 (2^24); larger n returns PHX_E_INVALID.  n == 0 writes *total = 0.
+ *   - stream: a cudaStream_t (0 = legacy default stream).  The call enqueues its work there and
+ *     then waits for that stream to finish, so the result is ready on return.
+ *   - the first call on each device looks up the scratch array's address (cudaGetSymbolAddress)
+ *     with that device current; make it before any stream capture on that device.
+ *   - calls share the one scratch array per device: two calls whose scans overlap on the GPU
+ *     (different streams, or different host threads) race on it and give wrong results.
+ * Returns PHX_E_TIMEOUT if a bounded look-back wait gave up (results then invalid). */
+PHX_API int phx_scan_noalloc(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *total, uint64_t stream);
+
 PHX_API const char *phx_last_error(void);
 PHX_API const char *phx_version(void);
 

@@ -173,6 +173,7 @@ PROTOTYPES = [
     ("phx_stage_ms", C.c_int, [VP, C.POINTER(C.c_float), C.c_uint32]),
     ("phx_get_stream", C.c_uint64, [VP]),
     ("phx_selftest_lookback_timeout", C.c_int, [C.c_int, C.c_uint32, C.POINTER(C.c_uint32)]),
+    ("phx_scan_noalloc", C.c_int, [VP, VP, C.c_uint32, VP, C.c_uint64]),
     ("phx_last_error", C.c_char_p, []),
     ("phx_version", C.c_char_p, []),
 ]

@@ -355,4 +355,20 @@ PHX_API int phx_selftest_lookback_timeout(int device, uint32_t n, uint32_t *err_
     });
 }
 
+PHX_API int phx_scan_noalloc(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *total, uint64_t stream) {
+    return guard([&]() -> int {
+        if (n && (!in || !out))
+            return fail(PHX_E_INVALID, "null buffer");
+        std::string msg;
+        int rc = scan_noalloc(in, out, n, total, (cudaStream_t)(uintptr_t)stream, msg);
+        if (rc == 1)
+            return fail(PHX_E_INVALID, msg);
+        if (rc == 3)
+            return fail(PHX_E_CUDA, msg);
+        if (rc == 4)
+            return fail(PHX_E_TIMEOUT, msg);
+        return PHX_OK;
+    });
+}
+
 } // extern "C"

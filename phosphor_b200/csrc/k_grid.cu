@@ -24,6 +24,8 @@
 #include "kernels.hpp"
 
 #include <cuda/atomic>
+#include <mutex>
+#include <string>
 
 namespace phx {
 
@@ -433,6 +435,88 @@ void launch_sorted_records(const u32 *perm, const float4 *ph_pos, const uint2 *p
         return;
     k_sorted_records<<<(unsigned)((n_max + 255) / 256), 256, 0, st>>>(perm, ph_pos, ph_pd, n_dev, s_posdir, s_power,
                                                                     n_max, err);
+}
+
+// ---- allocation-free exclusive scan --------------------------------------------------------------
+// Some callers cannot allocate device memory: hosts whose device memory is owned by a caching or
+// arena allocator that has reserved most of HBM (a side cudaMalloc fails or fragments it), plugins
+// whose host enforces a fixed memory budget, and latency-critical loops that may not pay
+// cudaMalloc/cudaFree's implicit device synchronisation after start-up.  For them the scan's
+// scratch — the tile ticket counter and one 8-byte look-back status word per 4096-element tile —
+// lives in this file-scope device array instead of a buffer the caller provides.  It is sized for
+// NOALLOC_SCAN_MAX_N elements (33,024 bytes per device, held by every GPU that loads the library
+// until the process exits).  All calls share it: each call clears it first, and two calls whose
+// kernels overlap on the GPU (different streams, or different host threads) race on it.
+constexpr u32 NOALLOC_SCAN_MAX_N = 1u << 24;
+constexpr u32 NOALLOC_SCAN_MAX_TILES = NOALLOC_SCAN_MAX_N / (u32)SCAN_TILE;
+constexpr size_t NOALLOC_SCRATCH_BYTES = 256 + 8 * (size_t)NOALLOC_SCAN_MAX_TILES;
+static __device__ __align__(256) unsigned char g_noalloc_scan_scratch[NOALLOC_SCRATCH_BYTES];
+
+// Host-side address of g_noalloc_scan_scratch on each device.  The array's name in host code is a
+// stand-in, not a device address, so the address is looked up once per device (with that device
+// current) through cudaGetSymbolAddress and passed to the kernel.  That set-up happens in the first
+// call on each device, which should therefore come before any stream capture on it.
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[128] = {};
+
+int scan_noalloc(const u32 *in, u32 *out, u32 n, u32 *total, cudaStream_t st, std::string &err) {
+    if (n > NOALLOC_SCAN_MAX_N) {
+        err = "n = " + std::to_string(n) + " exceeds the allocation-free scan's maximum of " +
+              std::to_string(NOALLOC_SCAN_MAX_N) + " elements";
+        return 1;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 128) {
+        err = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
+        return 3;
+    }
+    void *scr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void *p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
+            if (e != cudaSuccess || !p) {
+                err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+                return 3;
+            }
+            g_noalloc_ptr[dev] = p;
+        }
+        scr = g_noalloc_ptr[dev];
+    }
+    if (n == 0) {
+        if (total && (e = cudaMemsetAsync(total, 0, 4, st)) != cudaSuccess) {
+            err = std::string("cudaMemsetAsync: ") + cudaGetErrorString(e);
+            return 3;
+        }
+        return 0;
+    }
+    const u64 tiles = scan_tiles(n);
+    // ticket counter (offset 0), error word (offset 4) and the status words must start at zero
+    if ((e = cudaMemsetAsync(scr, 0, 256 + 8 * (size_t)tiles, st)) != cudaSuccess) {
+        err = std::string("cudaMemsetAsync: ") + cudaGetErrorString(e);
+        return 3;
+    }
+    u32 *counter = reinterpret_cast<u32 *>(scr);
+    u32 *errw = counter + 1;
+    u64 *status = reinterpret_cast<u64 *>(reinterpret_cast<char *>(scr) + 256);
+    k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, out, n, counter, status, total, errw);
+    if ((e = cudaGetLastError()) != cudaSuccess) {
+        err = std::string("scan launch: ") + cudaGetErrorString(e);
+        return 3;
+    }
+    u32 flags = 0;
+    if ((e = cudaMemcpyAsync(&flags, errw, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+        err = std::string("scan: ") + cudaGetErrorString(e);
+        return 3;
+    }
+    if (flags & ERR_LOOKBACK_TIMEOUT) {
+        err = "a decoupled look-back wait gave up";
+        return 4;
+    }
+    return 0;
 }
 
 // ---- one-time kernel set-up (outside any stream capture) ---------------------------------------

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 #include "dev_scene.cuh"
@@ -67,6 +68,9 @@ size_t scan_scratch_bytes(u64 n);
 void launch_scan(const u32 *in, u32 *out, u64 n, void *scratch, u32 *total, u32 *err, cudaStream_t st);
 // failure-detection self-test: scan with tile 0 withheld; returns 0 ok, 2 alloc, 3 CUDA error
 int selftest_lookback_timeout(int device, u32 n, u32 *err_out);
+// exclusive scan with its scratch in a static device array (no allocation); synchronous.
+// returns 0 ok, 1 too large, 3 CUDA error, 4 look-back timeout (message in err)
+int scan_noalloc(const u32 *in, u32 *out, u32 n, u32 *total, cudaStream_t st, std::string &err);
 
 // stable LSD radix sort of (key, canonical index) by key; n read from device *n_dev (<= n_max)
 size_t radix_scratch_bytes(u64 n_max, u32 key_bits);
