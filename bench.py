@@ -123,29 +123,35 @@ def make_args(cfg: dict, scale: int = 1):
                       grid_res=cfg["grid"], seed=1, sppm_alpha=0.7, direct_samples=16)
 
 
-def cpu_oracle_sample(cfg: dict, scale: int, rounds: int, threads: int) -> dict:
-    """The reference algorithm (oracle port, fp32) on the host cores: `rounds` SPPM rounds of the
-    workload at 1/scale of the resolution and 1/scale^2 of the photons (same scene)."""
+def cpu_oracle_sample(cfg: dict, threads: int, min_seconds: float = 10.0, max_rounds: int = 8) -> dict:
+    """The reference algorithm (oracle port, fp32) on the host cores, on the workload itself: one
+    untimed round, then whole rounds until `min_seconds` have passed (at most `max_rounds`)."""
     import oracle as O
     import phosphor_b200 as P
-    args = make_args(cfg, scale)
+    args = make_args(cfg, 1)
     scene = P.SceneData.generate(cfg["kind"], seed=1, width=args.width, height=args.height, detail=cfg["detail"])
     orc = O.Oracle(scene)
-    orc.render(args.params(), 1, prec=0, threads=threads)  # warm-up round
-    t0 = time.perf_counter()
-    st = orc.render(args.params(), rounds, prec=0, threads=threads)
-    dt = time.perf_counter() - t0
+    state = orc.render(args.params(), 1, prec=0, threads=threads)  # warm-up round
+    dt, rounds, stage = 0.0, 0, [0.0] * 4
+    while rounds < max_rounds and (rounds < 1 or dt < min_seconds):
+        t0 = time.perf_counter()
+        state = orc.render(args.params(), 1, prec=0, threads=threads, state=state)
+        dt += time.perf_counter() - t0
+        stage = [s + float(x) for s, x in zip(stage, state["seconds"])]
+        rounds += 1
     photons = args.photons_per_round * rounds
     return {"value": photons / dt / 1e6, "unit": METRIC, "cores": threads, "kind": "port",
-            "seconds": dt, "stage_seconds": [float(x) for x in st["seconds"]],
-            "sample": f"{rounds} SPPM round(s) at {args.width}x{args.height} px and {args.photons_per_round} "
-                      f"photons/round (1/{scale * scale} of the workload's pixels and photons, same scene), "
-                      f"fp32 oracle port of the reference kernels, {threads} threads"}
+            "seconds": dt, "stage_seconds": stage,
+            "sample": f"{rounds} SPPM round(s) of the workload itself ({args.width}x{args.height} px, "
+                      f"{args.photons_per_round} photons/round) after one untimed round, fp32 oracle port of the "
+                      f"reference kernels, {threads} threads"}
 
 
 def run_reference(a, cfg: dict) -> dict:
     threads = os.cpu_count() or 1
-    scale = 4
+    # each step is one whole round of the workload (about 3 s on 16 cores) unless that would make
+    # the run longer than a few minutes; then 1/scale of the resolution and 1/scale^2 of the photons
+    scale = 1 if a.steps + a.warmup <= 40 else 2 if a.steps + a.warmup <= 160 else 4
     import oracle as O
     import phosphor_b200 as P
     args = make_args(cfg, scale)
@@ -161,9 +167,10 @@ def run_reference(a, cfg: dict) -> dict:
         times.append(time.perf_counter() - t0)
     tot = sum(times)
     value = args.photons_per_round * a.steps / tot / 1e6
+    part = "the workload itself" if scale == 1 else f"1/{scale * scale} of the workload's pixels and photons"
     sample = (f"each step: one SPPM round at {args.width}x{args.height} px, {args.photons_per_round} photons "
-              f"(1/{scale * scale} of the workload's pixels and photons, same scene), fp32 oracle port of the "
-              f"reference kernels (no CPU OpenCL runtime exists for the reference's .cl), {threads} threads")
+              f"({part}, same scene), fp32 oracle port of the reference kernels (no CPU OpenCL runtime exists "
+              f"for the reference's .cl), {threads} threads")
     return {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * tot / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural scene)",
@@ -173,7 +180,8 @@ def run_reference(a, cfg: dict) -> dict:
 
 
 def algorithmic_bytes(stage: str, P: int, Ne: int, Ns: int, C: int, scene_bytes: int, ds: int = 16) -> int:
-    """Compulsory bytes per round of each stage (roofline table)."""
+    """Compulsory bytes per round of each stage: the hit-point, photon, cell and image records each
+    stage must read or write once, plus the scene geometry for the traversal stages."""
     return {
         "trace": 96 * P + 32 * P * ds + scene_bytes,
         "shadow": 48 * P * ds + 48 * P + scene_bytes,
@@ -307,7 +315,7 @@ def run_ours(a, cfg: dict) -> dict | None:
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cpu = cpu_oracle_sample(cfg, scale=4, rounds=1, threads=os.cpu_count() or 1)
+        cpu = cpu_oracle_sample(cfg, threads=os.cpu_count() or 1)
     r.close()
     if dist is not None:
         dist.destroy_process_group()
@@ -325,7 +333,7 @@ def run_ours(a, cfg: dict) -> dict | None:
 
 
 def run_batch16(a) -> dict:
-    """16 uneven scenes, all advanced per launch from one captured graph, against the
+    """The 16-scene batch workload: uneven scenes, all advanced per launch from one captured graph, against the
     plain per-pass form running the scenes one after another."""
     import torch
 

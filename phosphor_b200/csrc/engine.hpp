@@ -1,6 +1,6 @@
 // engine.hpp — device memory layout and stage orchestration for one or many scenes.
 //
-// HBM layout (all scenes concatenated in scene order, see DESIGN.md for sizes):
+// HBM layout (all scenes concatenated in scene order; sizes per buffer below):
 //   per pixel    hit point SoA: 6 x float4 (pos, normal, throughput, base colour, direct,
 //                emission) + SPPM state flux float4, weight f32, radiance float4   (132 B)
 //   per path     stored-photon count u32, exclusive offset u32

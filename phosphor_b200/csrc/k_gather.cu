@@ -39,41 +39,11 @@ PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
     float found = 0.0f;
     const u32 *cs = g.cell_start + sc.cell_base;
     const float denom = 2.0f * r_sq;
-    // The 27 cells x their photons, flattened into one sequence per pixel in the reference's order
-    // (cell i = 0..26, photons in cell order): each iteration of the warp-synchronous loop moves
-    // every lane one step along its own sequence, so lanes with short and long cells stay busy.
-    u32 i = 0, k = 0, end = 0; // current cell index, photon cursor, end of the current cell
-    const u32 mask = __activemask();
-    bool more = true;
-    while (__any_sync(mask, more)) {
-        if (!more)
-            continue;
-        if (k >= end) { // advance to the next non-empty cell (photon_hash.h:65-82)
-            for (;;) {
-                if (i >= 27) {
-                    more = false;
-                    break;
-                }
-                const i32 cx = (i32)(i % 3) - 1;
-                const i32 cy = (i32)((i / 3) % 3) - 1;
-                const i32 cz = (i32)((i / 9) % 3) - 1;
-                float px = pos.x, py = pos.y, pz = pos.z;
-                px += (float)cx * grid.cx;
-                py += (float)cy * grid.cy;
-                pz += (float)cz * grid.cz;
-                const u32 h = get_hash(px, py, pz, grid);
-                i++;
-                if (h == 0)
-                    continue;
-                k = min(__ldg(&cs[h]), g.n_cap);
-                end = min(__ldg(&cs[h + 1]), g.n_cap);
-                if (k < end)
-                    break;
-            }
-            if (!more)
-                continue;
-        }
-        const float4 p = __ldg(&g.s_posdir[k]);
+    // hit point in cell units, for the cell-distance test below
+    const float qx = (pos.x - grid.ox) / grid.cx, qy = (pos.y - grid.oy) / grid.cy, qz = (pos.z - grid.oz) / grid.cz;
+    const u32 G = grid.g;
+    // One photon's contribution, in the reference's arithmetic (photon_hash.h:84-101).
+    auto add = [&](const float4 p, u32 k) {
         const float dx = pos.x - p.x, dy = pos.y - p.y, dz = pos.z - p.z, dw = pos.w - 0.0f;
         const float dsq = ((dx * dx + dy * dy) + dz * dz) + dw * dw;
         if (dsq < r_sq) {
@@ -84,7 +54,41 @@ PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
                 found += w;
             }
         }
-        k++;
+    };
+    // The 27 cells in the reference's order (photon_hash.h:65-82), each in sorted (canonical)
+    // photon order.  A cell whose box lies farther than the search radius from the hit point holds
+    // no photon with dsq < r_sq, so it adds nothing and is skipped; the box is widened by 1/1024
+    // of a cell on every side so that rounding in get_hash (which decides a photon's cell) and in
+    // this test can never skip a photon that would count.
+    constexpr float M = 1.0f / 1024.0f;
+    for (u32 i = 0; i < 27; i++) {
+        const i32 ox = (i32)(i % 3) - 1;
+        const i32 oy = (i32)((i / 3) % 3) - 1;
+        const i32 oz = (i32)((i / 9) % 3) - 1;
+        float px = pos.x, py = pos.y, pz = pos.z;
+        px += (float)ox * grid.cx;
+        py += (float)oy * grid.cy;
+        pz += (float)oz * grid.cz;
+        const u32 h = get_hash(px, py, pz, grid);
+        if (h == 0)
+            continue;
+        const u32 hz = (h - 1) % G, hy = ((h - 1) / G) % G, hx = (h - 1) / (G * G);
+        const float gx = fmaxf(fmaxf(((float)hx - M) - qx, qx - ((float)hx + (1.0f + M))), 0.0f) * grid.cx;
+        const float gy = fmaxf(fmaxf(((float)hy - M) - qy, qy - ((float)hy + (1.0f + M))), 0.0f) * grid.cy;
+        const float gz = fmaxf(fmaxf(((float)hz - M) - qz, qz - ((float)hz + (1.0f + M))), 0.0f) * grid.cz;
+        if ((gx * gx + gy * gy) + gz * gz > r_sq)
+            continue;
+        u32 k = min(__ldg(&cs[h]), g.n_cap);
+        const u32 end = min(__ldg(&cs[h + 1]), g.n_cap);
+        // two records in flight per step; contributions still added in photon order
+        for (; k + 1 < end; k += 2) {
+            const float4 p0 = __ldg(&g.s_posdir[k]);
+            const float4 p1 = __ldg(&g.s_posdir[k + 1]);
+            add(p0, k);
+            add(p1, k + 1);
+        }
+        if (k < end)
+            add(__ldg(&g.s_posdir[k]), k);
     }
     if (found > 0.0f) {
         float nw = wso + sc.alpha * found;
