@@ -127,10 +127,19 @@ def rounds_to_target(specs, refs, target: float, max_rounds: int, check_every: i
     return r_star, curve
 
 
-def time_plain(spec: SceneSpec, rounds: int, device: int = 0) -> float:
-    """Seconds per round of one scene in the plain per-pass form (host wall clock)."""
-    r = Renderer(spec.args(), device=device)
+def time_plain(spec: SceneSpec, rounds: int, device: int = 0, reference_shaped: bool = False) -> float:
+    """Seconds per round of one scene in the plain per-pass form (host wall clock).  With
+    `reference_shaped`, the kernels also take the reference's shape: one thread per pixel / photon
+    path, the reference's median-split tree with its stack traversal, NEE inline in the camera pass."""
+    args = spec.args()
+    if reference_shaped:
+        args.flags = A.PHX_F_SIMPLE_TRAVERSAL | A.PHX_F_REFERENCE_BVH
+    r = Renderer(args, device=device)
     r.set_scene(spec.scene())
+    if reference_shaped:
+        t = r.tuning()
+        t.persistent, t.nee_wavefront = 0, 0
+        r.set_tuning(t)
     r.round()
     t0 = time.perf_counter()
     for _ in range(rounds):
