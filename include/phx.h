@@ -327,6 +327,35 @@ PHX_API int phx_stage_ms(void *ctx, float *out, uint32_t n);
 /* The CUDA stream (cudaStream_t) every stage of the context or batch is enqueued on. */
 PHX_API uint64_t phx_get_stream(void *ctx);
 
+/* ---- differentiation (single-scene contexts) -------------------------------------------------------
+ * No counterpart in the reference.  Parameters θ: per material its base colour (r, g, b) and
+ * roughness, per light its power (r, g, b); gradients are laid out as 4 floats per material
+ * (base r, g, b, roughness) followed by 3 per light (power r, g, b).
+ * What is differentiated is the frozen-path estimator of the image: every random or discrete choice
+ * of the forward render (paths, BSDF events, microfacet normals, Russian roulette, light selection,
+ * gather neighbourhoods, kernel weights, radii, SPPM ratios) is held fixed and only the weights move
+ * with θ — a BSDF bounce weighs W(θ0)·f(θ)/f(θ0) along its frozen directions, light power enters
+ * linearly and photon power is taken unquantised.  The gradient is exact for that function (up to
+ * float rounding); the oracle evaluates the same function in double for finite-difference checks.
+ * Paths are replayed from their RNG seeds in the backward pass; nothing per vertex is stored.
+ * A gradient with respect to a base-colour channel or light-power channel whose current value is 0,
+ * or a roughness at its clamp (0.001 or 1), is reported as 0. */
+/* Replaces the material table (same count; texture indices unchanged). */
+PHX_API int phx_set_materials(void *ctx, const phx_material *materials, uint32_t n);
+/* Replaces the lights (same count and kinds); the light-selection CDF is rebuilt
+ * (scene_data.cpp:14-23). */
+PHX_API int phx_set_lights(void *ctx, const phx_light *lights, uint32_t n);
+/* Number of parameters: 4 * materials + 3 * lights. */
+PHX_API int phx_adjoint_n_params(void *ctx, uint32_t *n);
+/* Clears the SPPM state, renders `rounds` rounds (1..4096) recording what the backward pass needs,
+ * and writes the linear image radiance/R + flux/(π r² N) (width*height*3 floats, before exposure and
+ * gamma) to `image` (may be NULL). */
+PHX_API int phx_adjoint_forward(void *ctx, uint32_t rounds, float *image);
+/* Gradient of L with respect to θ given dL/dI (width*height*3 floats, same layout as the image) for
+ * the last phx_adjoint_forward; n_grad >= phx_adjoint_n_params.  PHX_E_STATE if a round, gather,
+ * buffer write or parameter change came in between.  May be called again with another dL/dI. */
+PHX_API int phx_adjoint_backward(void *ctx, const float *dl_dimage, float *grad, uint32_t n_grad);
+
 /* ---- failure detection self-test ----------------------------------------------------------------
  * Runs the decoupled look-back scan over n elements with tile 0 withheld (the tile ticket counter
  * starts at 1), so every other tile waits on a predecessor that never publishes.  The bounded

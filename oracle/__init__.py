@@ -52,6 +52,7 @@ def load() -> C.CDLL:
         "orc_decode_oct": (None, [vp, C.c_uint32, vp]),
         "orc_get_hash": (None, [vp, C.c_uint32, vp, vp]),
         "orc_math": (C.c_float, [C.c_int, C.c_float, C.c_float]),
+        "orc_frozen_render": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, vp, C.c_uint32, C.c_int, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -143,6 +144,22 @@ class Oracle:
         state["n_last"] = n_last.value
         state["seconds"] = secs
         return state
+
+    def frozen_render(self, params, rounds: int, materials: np.ndarray, lights: np.ndarray,
+                      threads: int | None = None):
+        """The frozen-path estimator F(θ') of phx_frozen.hpp: paths and all decisions from this
+        scene's own materials and lights (θ0), weights from `materials` / `lights` (θ', arrays of
+        phx_material / phx_light records in the scene's order).  Returns (image (npx, 3) float64
+        linear radiance, θ0 flux (npx, 4) float32, θ0 radiance (npx, 4) float32)."""
+        npx = params.width * params.height
+        img = np.empty((npx, 3), dtype=np.float64)
+        flux = np.empty((npx, 4), dtype=np.float32)
+        rad = np.empty((npx, 4), dtype=np.float32)
+        mats = np.ascontiguousarray(materials)
+        lts = np.ascontiguousarray(lights)
+        _chk(self.lib.orc_frozen_render(self.h, C.addressof(params), rounds, _p(mats), len(mats), _p(lts), len(lts),
+                                        threads or default_threads(), _p(img), _p(flux), _p(rad)))
+        return img, flux, rad
 
 
 def bvh_build(tris_ptr, n: int):

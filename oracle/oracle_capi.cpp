@@ -1,6 +1,7 @@
 // oracle_capi.cpp — TEST INFRASTRUCTURE ONLY: extern "C" entry points of the CPU oracle
 // (liboracle.so), called through ctypes by tests/ and by bench.py's CPU-baseline leg.
 // PARITY UNPINNED BY THE REFERENCE (see phx_oracle.hpp).
+#include "phx_frozen.hpp"
 #include "phx_oracle.hpp"
 
 #include <atomic>
@@ -35,6 +36,7 @@ void parallel_for(uint32_t n, int threads, const std::function<void(uint32_t, ui
 
 struct OrcCtx {
     Scene sc;
+    u32 n_materials = 0;
     std::vector<phx_bvh_node> bvh;
     u32 depth = 0;
 };
@@ -261,6 +263,83 @@ int render_impl(OrcCtx *o, const phx_params *p, u32 rounds, int threads, void *f
     return PHX_OK;
 }
 
+// The frozen-path estimator F(θ') (phx_frozen.hpp) over `rounds` rounds from a fresh state:
+// linear image (radiance/R + flux/(π r² N)) in double into img1 (npx x 3); the θ0 float state
+// (bit-identical to render_impl<float>) into flux0/radiance0 when given.
+int frozen_render_impl(OrcCtx *o, const phx_params *p, u32 rounds, const frozen::Primed &pr, int threads,
+                       double *img1, float *flux0, float *radiance0) {
+    using frozen::D4;
+    u32 npx = p->width * p->height;
+    u32 buckets = p->grid_res * p->grid_res * p->grid_res + 1;
+    u32 maxb = p->max_photon_bounces, ne = p->photons_per_round;
+    phx_photon_hash_data hd = hash_info(o->bvh[0], p->grid_res);
+    std::vector<HitPoint<float>> hp(npx);
+    std::vector<frozen::HitPrimed> hp1(npx);
+    std::vector<StoredPhoton<float>> slots((size_t)ne * maxb);
+    std::vector<D4> slot_pow1((size_t)ne * maxb);
+    std::vector<u32> cnt(ne);
+    std::vector<V4<float>> flux(npx, zero4<float>()), radiance(npx, zero4<float>());
+    std::vector<float> weight(npx, 0.0f);
+    std::vector<D4> flux1(npx, zero4<double>()), rad1(npx, zero4<double>());
+    std::vector<u32> counts(buckets), start(buckets), end(buckets);
+    Rng rng = pcg_seed(p->seed);
+    for (u32 round = 0; round < rounds; round++) {
+        u32 seed = random_u32(&rng);
+        parallel_for(npx, threads, [&](u32 b, u32 e) {
+            for (u32 i = b; i < e; i++)
+                hp[i] = frozen::trace_pixel(o->sc, pr, p->width, p->height, seed, p->direct_samples, i, &hp1[i]);
+        });
+        parallel_for(ne, threads, [&](u32 b, u32 e) {
+            for (u32 i = b; i < e; i++)
+                cnt[i] = frozen::emit_photon(o->sc, pr, i, maxb, seed, &slots[(size_t)i * maxb],
+                                             &slot_pow1[(size_t)i * maxb]);
+        });
+        std::vector<float> pos;
+        std::vector<u32> power, dir;
+        std::vector<D4> pow1;
+        for (u32 i = 0; i < ne; i++) // canonical order: path, then bounce
+            for (u32 j = 0; j < cnt[i]; j++) {
+                const StoredPhoton<float> &s = slots[(size_t)i * maxb + j];
+                pos.insert(pos.end(), {s.pos.x, s.pos.y, s.pos.z, s.pos.w});
+                power.push_back(s.power);
+                dir.push_back(s.dir);
+                pow1.push_back(slot_pow1[(size_t)i * maxb + j]);
+            }
+        u32 n = (u32)power.size();
+        if (n == 0)
+            return PHX_E_NO_PHOTONS;
+        std::vector<u32> keys(n), spower(n), sdir(n), perm(n);
+        std::vector<float> spos((size_t)n * 4);
+        hash_impl<float>(pos.data(), n, hd, buckets, keys.data(), counts.data());
+        reference_scan(counts.data(), buckets, start.data());
+        scatter_impl<float>(pos.data(), power.data(), dir.data(), keys.data(), n, start.data(), buckets, spos.data(),
+                            spower.data(), sdir.data(), end.data(), perm.data());
+        std::vector<D4> spow1(n);
+        for (u32 k = 0; k < n; k++)
+            spow1[k] = pow1[perm[k]];
+        const V4<float> *sp = (const V4<float> *)spos.data();
+        parallel_for(npx, threads, [&](u32 b, u32 e) {
+            for (u32 i = b; i < e; i++)
+                frozen::gather_pixel(hp[i], hp1[i], hd, start.data(), end.data(), sp, spower.data(), sdir.data(),
+                                     spow1.data(), p->sppm_alpha, &flux[i], &weight[i], &radiance[i], &flux1[i],
+                                     &rad1[i]);
+        });
+    }
+    const double n_total = (double)p->photons_per_round * rounds;
+    for (u32 i = 0; i < npx; i++) {
+        const double area = (double)PI_F * flux[i].w;
+        const double per = area > 0.0 ? 1.0 / (area * n_total) : 0.0;
+        img1[3 * (size_t)i + 0] = rad1[i].x / rounds + flux1[i].x * per;
+        img1[3 * (size_t)i + 1] = rad1[i].y / rounds + flux1[i].y * per;
+        img1[3 * (size_t)i + 2] = rad1[i].z / rounds + flux1[i].z * per;
+        if (flux0)
+            store4<float>(flux0, i, flux[i]);
+        if (radiance0)
+            store4<float>(radiance0, i, radiance[i]);
+    }
+    return PHX_OK;
+}
+
 // output.cpp:40-83 in float (u8 quantisation left to the caller)
 template <class R>
 void image_impl(const void *flux, const void *radiance, u32 n, float exposure, int tonemap, uint64_t total_photons,
@@ -325,6 +404,7 @@ __attribute__((visibility("default"))) void *orc_create(const phx_scene *s) {
     sc.etris = s->emissive_triangles;
     sc.n_etris = s->n_emissive_triangles;
     sc.materials = s->materials;
+    o->n_materials = s->n_materials;
     sc.uv = s->uv_transforms;
     sc.lights = s->lights;
     sc.n_lights = s->n_lights;
@@ -412,6 +492,20 @@ __attribute__((visibility("default"))) int orc_render(void *o, const phx_params 
                                    stage_seconds);
     return render_impl<float>((OrcCtx *)o, p, rounds, threads, flux4, weight, radiance4, total_emitted, n_last,
                               stage_seconds);
+}
+
+/* F(θ') of phx_frozen.hpp: mats1 / lights1 are θ' (the scene's counts), img1 npx x 3 doubles */
+__attribute__((visibility("default"))) int orc_frozen_render(void *o, const phx_params *p, uint32_t rounds,
+                                                            const phx_material *mats1, uint32_t n_mats,
+                                                            const phx_light *lights1, uint32_t n_lights,
+                                                            int threads, double *img1, float *flux4,
+                                                            float *radiance4) {
+    auto *c = (OrcCtx *)o;
+    if (!c || !p || !img1 || rounds == 0 || n_mats != c->n_materials || n_lights != c->sc.n_lights ||
+        (n_mats && !mats1) || (n_lights && !lights1))
+        return PHX_E_INVALID;
+    frozen::Primed pr{mats1, lights1};
+    return frozen_render_impl(c, p, rounds, pr, threads, img1, flux4, radiance4);
 }
 
 __attribute__((visibility("default"))) int orc_image(const void *flux4, const void *radiance4, uint32_t n, int prec,

@@ -174,6 +174,11 @@ PROTOTYPES = [
     ("phx_get_stream", C.c_uint64, [VP]),
     ("phx_selftest_lookback_timeout", C.c_int, [C.c_int, C.c_uint32, C.POINTER(C.c_uint32)]),
     ("phx_scan_noalloc", C.c_int, [VP, VP, C.c_uint32, VP, C.c_uint64]),
+    ("phx_set_materials", C.c_int, [VP, VP, C.c_uint32]),
+    ("phx_set_lights", C.c_int, [VP, VP, C.c_uint32]),
+    ("phx_adjoint_n_params", C.c_int, [VP, C.POINTER(C.c_uint32)]),
+    ("phx_adjoint_forward", C.c_int, [VP, C.c_uint32, VP]),
+    ("phx_adjoint_backward", C.c_int, [VP, VP, VP, C.c_uint32]),
     ("phx_last_error", C.c_char_p, []),
     ("phx_version", C.c_char_p, []),
 ]

@@ -103,7 +103,8 @@ def build_cli(force: bool = False, verbose: bool = False) -> Path:
 def build_oracle(force: bool = False, verbose: bool = False) -> Path:
     """Compiles the CPU oracle (test infrastructure only; see oracle/phx_oracle.hpp)."""
     srcs = [ORACLE_DIR / "oracle_capi.cpp"]
-    deps = srcs + [ORACLE_DIR / "phx_oracle.hpp", INCLUDE / "phx.h", INCLUDE / "phx_math.h"]
+    deps = srcs + [ORACLE_DIR / "phx_oracle.hpp", ORACLE_DIR / "phx_frozen.hpp", INCLUDE / "phx.h",
+                   INCLUDE / "phx_math.h"]
     if not force and ORACLE_LIB.exists() and ORACLE_LIB.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
         return ORACLE_LIB
     tmp = ORACLE_LIB.with_suffix(".so.tmp")

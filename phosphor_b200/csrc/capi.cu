@@ -355,6 +355,37 @@ PHX_API int phx_selftest_lookback_timeout(int device, uint32_t n, uint32_t *err_
     });
 }
 
+PHX_API int phx_set_materials(void *ctx, const phx_material *materials, uint32_t n) {
+    return guard([&]() -> int {
+        return ctx ? eng(ctx)->set_materials(materials, n) : fail(PHX_E_INVALID, "null context");
+    });
+}
+
+PHX_API int phx_set_lights(void *ctx, const phx_light *lights, uint32_t n) {
+    return guard([&]() -> int { return ctx ? eng(ctx)->set_lights(lights, n) : fail(PHX_E_INVALID, "null context"); });
+}
+
+PHX_API int phx_adjoint_n_params(void *ctx, uint32_t *n) {
+    return guard([&]() -> int {
+        if (!ctx || !n)
+            return fail(PHX_E_INVALID, "null argument");
+        *n = eng(ctx)->n_params();
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_adjoint_forward(void *ctx, uint32_t rounds, float *image) {
+    return guard([&]() -> int {
+        return ctx ? eng(ctx)->adjoint_forward(rounds, image) : fail(PHX_E_INVALID, "null context");
+    });
+}
+
+PHX_API int phx_adjoint_backward(void *ctx, const float *dl_dimage, float *grad, uint32_t n_grad) {
+    return guard([&]() -> int {
+        return ctx ? eng(ctx)->adjoint_backward(dl_dimage, grad, n_grad) : fail(PHX_E_INVALID, "null context");
+    });
+}
+
 PHX_API int phx_scan_noalloc(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *total, uint64_t stream) {
     return guard([&]() -> int {
         if (n && (!in || !out))

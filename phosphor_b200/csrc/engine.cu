@@ -62,7 +62,8 @@ Engine::~Engine() {
                      &d_err, &d_ovf, &d_queue, &d_ntotal,
                      &flux, &weight, &radiance, &slot_pos, &slot_pd, &counts, &offsets, &ph_pos, &ph_pd, &keys,
                      &cell_count, &cell_start, &sk0, &sk1, &sv0, &sv1, &s_posdir, &s_power, &scan_scr, &radix_scr,
-                     &img_rgb, &img_ldr};
+                     &img_rgb, &img_ldr, &adj_seeds, &adj_r2, &adj_ratio, &adj_k, &adj_img, &adj_g, &adj_gT,
+                     &adj_gA, &adj_gphi, &adj_slot_pow, &adj_ph_pow, &adj_grad};
     for (auto *b : all)
         b->release();
     for (auto &b : hp)
@@ -219,6 +220,8 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
                     has_env ? (size_t)s.envmap_width * s.envmap_height * 3 * 4 : 16)))
         return r;
 
+    S.mats.assign(s.materials, s.materials + s.n_materials);
+    S.lights.assign(s.lights, s.lights + s.n_lights);
     SceneDesc &d = S.desc;
     std::memset(&d, 0, sizeof(d));
     d.cnodes = S.bufs[0].as<float4>();
@@ -465,11 +468,12 @@ void Engine::enq_hash_sort() {
 }
 
 void Engine::enq_gather() {
+    adjoint_invalidate();
     ev(ST_GATHER, false);
     GatherBufs g{hp[0].as<float4>(), hp[1].as<float4>(), hp[2].as<float4>(), hp[3].as<float4>(),
                  hp[4].as<float4>(), hp[5].as<float4>(), s_posdir.as<float4>(), s_power.as<u32>(),
                  cell_start.as<u32>(), (u32)max_photons, flux.as<float4>(), weight.as<float>(),
-                 radiance.as<float4>()};
+                 radiance.as<float4>(), rec_r2, rec_ratio};
     launch_gather(lc(), g, (int)tune.gather_block, st);
     ev(ST_GATHER, true);
 }
@@ -631,6 +635,7 @@ void Engine::count_round(uint32_t rounds) {
 }
 
 int Engine::graph_rounds(uint32_t rounds) {
+    adjoint_invalidate();
     int r;
     if (!gexec && (r = capture(true, &graph, &gexec)))
         return r;
@@ -655,6 +660,7 @@ int Engine::graph_rounds(uint32_t rounds) {
 }
 
 int Engine::seeded_round(uint32_t seed) {
+    adjoint_invalidate();
     int r;
     if (!gexec_host && (r = capture(false, &graph_host, &gexec_host)))
         return r;
@@ -675,12 +681,7 @@ int Engine::seeded_round(uint32_t seed) {
     return PHX_OK;
 }
 
-int Engine::set_alpha(float alpha) {
-    CK(cudaStreamSynchronize(st));
-    for (auto &s : sc) {
-        s.desc.alpha = alpha;
-        s.prm.sppm_alpha = alpha;
-    }
+int Engine::upload_descs() {
     std::vector<SceneDesc> d(sc.size());
     for (size_t i = 0; i < sc.size(); i++)
         d[i] = sc[i].desc;
@@ -688,7 +689,18 @@ int Engine::set_alpha(float alpha) {
     return PHX_OK;
 }
 
+int Engine::set_alpha(float alpha) {
+    adjoint_invalidate();
+    CK(cudaStreamSynchronize(st));
+    for (auto &s : sc) {
+        s.desc.alpha = alpha;
+        s.prm.sppm_alpha = alpha;
+    }
+    return upload_descs();
+}
+
 int Engine::set_n_photons(uint32_t n) {
+    adjoint_invalidate();
     if (sc.size() != 1)
         return fail(PHX_E_UNSUPPORTED, "photon injection is only available on single-scene contexts");
     if (n > max_photons)
@@ -844,6 +856,7 @@ int Engine::read_buffer(uint32_t s, int which, void *dst, uint64_t off, uint64_t
 }
 
 int Engine::write_buffer(uint32_t s, int which, const void *src, uint64_t off, uint64_t bytes) {
+    adjoint_invalidate();
     if (sc.size() != 1 || s != 0)
         return fail(PHX_E_UNSUPPORTED, "buffer writes are only available on single-scene contexts");
     if (!src && bytes)

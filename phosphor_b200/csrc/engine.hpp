@@ -40,6 +40,8 @@ struct SceneSlot {
     uint64_t total_emitted = 0;
     uint32_t rounds = 0;
     uint32_t n_photons_last = 0;
+    std::vector<phx_material> mats; // host copies of the parameters the adjoint differentiates
+    std::vector<phx_light> lights;
 };
 
 enum Stage {
@@ -86,6 +88,17 @@ class Engine {
     void stage_ms(float *out) const;
     void invalidate_graph();
 
+    // differentiation (single-scene engines; engine_adjoint.cu)
+    int set_materials(const phx_material *m, uint32_t n);
+    int set_lights(const phx_light *l, uint32_t n);
+    uint32_t n_params() const;
+    int adjoint_forward(uint32_t rounds, float *image);
+    int adjoint_backward(const float *dl_dimage, float *grad, uint32_t n_grad);
+    void adjoint_invalidate() {
+        if (!in_adjoint)
+            adj_ready = false;
+    }
+
     int device = 0;
     cudaStream_t st = nullptr;
     std::vector<SceneSlot> sc;
@@ -111,6 +124,14 @@ class Engine {
     DevBuf sk0, sk1, sv0, sv1, s_posdir, s_power, scan_scr, radix_scr, img_rgb, img_ldr;
     int capture(bool with_seeds, cudaGraph_t *g, cudaGraphExec_t *ge);
     void count_round(uint32_t rounds);
+
+    int upload_descs();
+    // adjoint state: per round seeds, search radii² and SPPM ratios of the forward pass
+    DevBuf adj_seeds, adj_r2, adj_ratio, adj_k, adj_img, adj_g, adj_gT, adj_gA, adj_gphi, adj_slot_pow, adj_ph_pow,
+        adj_grad;
+    uint32_t adj_rounds = 0;
+    bool adj_ready = false, adj_k_ready = false, in_adjoint = false;
+    float *rec_r2 = nullptr, *rec_ratio = nullptr; // recording targets of the gather (forward pass)
 
     u32 *perm = nullptr;
     u32 *h_pinned = nullptr;

@@ -60,6 +60,8 @@ PHX_DI u32 emit_path(const SceneDesc &sc, u32 seed, u32 tid, const EmitOut &out,
         if (bs.event == BSDF_DIFFUSE && dot(dir, sh.normal) < 0.0f) {
             out.slot_pos[slot] = sh.position;
             out.slot_pd[slot] = make_uint2(encode_rgbe(power), encode_oct(dir));
+            if (out.slot_pow)
+                out.slot_pow[slot] = power;
             slot += stride;
             n_out++;
         }
@@ -199,7 +201,7 @@ void launch_emit(const LaunchCtx &lc, const EmitOut &out, int block, int persist
                  cudaStream_t st) {
     if (lc.total_emit == 0)
         return;
-    if (persistent && queue) {
+    if (persistent && queue && !out.slot_pow) {
         cudaMemsetAsync(queue, 0, sizeof(u32), st);
         int grid = g_sm_count * (blocks_per_sm > 0 ? blocks_per_sm : 8);
         k_emit_persistent<<<grid, 128, 0, st>>>(lc, out, queue);

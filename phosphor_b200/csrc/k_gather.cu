@@ -18,6 +18,10 @@ PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
     float4 r = f4(ge.x, ge.y, ge.z, 0.0f);
     if (ge.w == 0.0f) {
         g.radiance[gpix] = rso + r;
+        if (g.rec_r2) {
+            g.rec_r2[gpix] = 0.0f;
+            g.rec_ratio[gpix] = 1.0f;
+        }
         return;
     }
     float4 direct = g.hp_direct[gpix];
@@ -89,6 +93,10 @@ PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
         }
         if (k < end)
             add(__ldg(&g.s_posdir[k]), k);
+    }
+    if (g.rec_r2) {
+        g.rec_r2[gpix] = r_sq;
+        g.rec_ratio[gpix] = found > 0.0f ? (wso + sc.alpha * found) / (wso + found) : 1.0f;
     }
     if (found > 0.0f) {
         float nw = wso + sc.alpha * found;

@@ -42,8 +42,9 @@ void launch_nee_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t s
 
 struct EmitOut {
     float4 *slot_pos;
-    uint2 *slot_pd; // (rgbe power, octahedral direction)
-    u32 *counts;    // per photon path (global emit index)
+    uint2 *slot_pd;    // (rgbe power, octahedral direction)
+    u32 *counts;       // per photon path (global emit index)
+    float4 *slot_pow;  // optional (one-thread-per-path form only): unquantised power per slot
 };
 void launch_emit(const LaunchCtx &lc, const EmitOut &out, int block, int persistent, int blocks_per_sm, u32 *queue,
                  cudaStream_t st);
@@ -90,8 +91,35 @@ struct GatherBufs {
     float4 *flux;
     float *weight;
     float4 *radiance;
+    float *rec_r2;         // optional: per pixel, the search radius² used this round
+    float *rec_ratio;      // optional: per pixel, the SPPM ratio applied to the flux (1 if none)
 };
 void launch_gather(const LaunchCtx &lc, const GatherBufs &g, int block, cudaStream_t st);
+
+// adjoint (single scene): gather adjoint, camera / photon path replays, helpers
+struct AdjBufs {
+    const float4 *g_img;   // dL/dI per pixel (linear radiance; .w unused)
+    const float *kscale;   // K_n per pixel for the round being replayed
+    const float *r2;       // search radius² per pixel in that round
+    float4 *gT, *gA;       // dL/d throughput and dL/d base colour of each hit point
+    float4 *gphi;          // dL/d power per canonical photon
+    const float4 *ph_pow;  // unquantised power per canonical photon
+    const u32 *perm;       // cell-order index -> canonical index
+    const u32 *offsets;    // first canonical photon of each path (total_emit + 1 entries)
+    double *grad;          // 4 per material (base r, g, b, roughness), then 3 per light (power r, g, b)
+    u32 n_params, n_mat;
+    float inv_rounds;
+    u32 block_sums;        // 1: per-block partial sums in 4*n_params bytes of shared memory
+};
+void launch_gather_adj(const LaunchCtx &lc, const GatherBufs &g, const AdjBufs &ab, cudaStream_t st);
+void launch_trace_adj(const LaunchCtx &lc, const AdjBufs &ab, cudaStream_t st);
+void launch_emit_adj(const LaunchCtx &lc, const AdjBufs &ab, cudaStream_t st);
+void launch_compact_pow(const LaunchCtx &lc, const float4 *slot_pow, const u32 *counts, const u32 *offsets,
+                        float4 *ph_pow, cudaStream_t st);
+void launch_adj_scale(const float *ratio, float *kscale, const float4 *flux, u32 n_pix, u32 rounds, float inv_n,
+                      cudaStream_t st);
+void launch_adj_image(const float4 *flux, const float4 *radiance, u32 n_pix, float inv_rounds, float inv_n, float *img,
+                      cudaStream_t st);
 
 // image formation (output.cpp:52-83) for one scene's pixel range
 void launch_image(const float4 *flux, const float4 *radiance, u32 n, float exposure, int tonemap, float inv_photons,

@@ -298,6 +298,39 @@ class Renderer:
     def stream(self) -> int:
         return int(self._lib.phx_get_stream(self._need()))
 
+    # differentiation (no reference counterpart; see include/phx.h)
+    def n_params(self) -> int:
+        n = C.c_uint32()
+        A.check(self._lib.phx_adjoint_n_params(self._need(), C.byref(n)))
+        return n.value
+
+    def set_materials(self, materials: np.ndarray) -> None:
+        """Replaces the material table (phx_material records, the scene's count and order)."""
+        m = np.ascontiguousarray(materials)
+        A.check(self._lib.phx_set_materials(self._need(), m.ctypes.data, len(m)))
+
+    def set_lights(self, lights: np.ndarray) -> None:
+        lt = np.ascontiguousarray(lights)
+        A.check(self._lib.phx_set_lights(self._need(), lt.ctypes.data, len(lt)))
+
+    def adjoint_forward(self, rounds: int) -> np.ndarray:
+        """Fresh render of `rounds` rounds recorded for the adjoint; linear image (H, W, 3)."""
+        a = self.args
+        img = np.empty((a.height, a.width, 3), dtype=np.float32)
+        A.check(self._lib.phx_adjoint_forward(self._need(), rounds, img.ctypes.data))
+        return img
+
+    def adjoint_backward(self, dl_dimage: np.ndarray) -> np.ndarray:
+        """dL/dθ (4 per material: base r, g, b, roughness; 3 per light: power r, g, b)."""
+        g = np.ascontiguousarray(dl_dimage, dtype=np.float32)
+        a = self.args
+        if g.size != a.width * a.height * 3:
+            raise ValueError("dL/dI must have width*height*3 entries")
+        n = self.n_params()
+        out = np.empty(n, dtype=np.float32)
+        A.check(self._lib.phx_adjoint_backward(self._need(), g.ctypes.data, out.ctypes.data, n))
+        return out
+
 
 class Batch:
     """Many scenes advanced together: one launch per stage for all scenes (phx_batch_*)."""
