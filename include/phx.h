@@ -297,6 +297,10 @@ PHX_API int phx_batch_destroy(void *batch);
 /* mode 0: plain form, scenes one at a time with per-pass launches and host syncs;
  * mode 1: all scenes per launch, each round replayed from a captured CUDA graph. */
 PHX_API int phx_batch_iterate(void *batch, uint32_t rounds, int mode);
+/* Retires (active = 0) or resumes a scene of the batch: every stage skips a retired scene, its
+ * state and round count stay as they are, and the captured graph stays valid.  No counterpart in
+ * the reference (a scene that has converged stops costing work in the batched form). */
+PHX_API int phx_batch_set_active(void *batch, uint32_t scene, int active);
 PHX_API int phx_batch_read_buffer(void *batch, uint32_t scene, int which, void *dst, uint64_t offset_bytes,
                                   uint64_t bytes);
 PHX_API int phx_batch_get_info(void *batch, uint32_t scene, phx_info *out);
@@ -311,7 +315,9 @@ typedef struct phx_tuning {
     uint32_t emit_blocks_per_sm;
     uint32_t persistent;        /* 1 = persistent lane-refill kernels, 0 = one thread per item */
     uint32_t nee_wavefront;     /* 1 = diffuse-hit NEE shadow rays traced by a separate wavefront */
-    uint32_t reserved[5];
+    uint32_t concurrent_passes; /* 1 = in the captured graph the camera pass and the photon pass of a
+                                   round run on two branches (they only share the round seed) */
+    uint32_t reserved[4];
 } phx_tuning;
 PHX_API int phx_get_tuning(void *ctx, phx_tuning *out);
 PHX_API int phx_set_tuning(void *ctx, const phx_tuning *in);

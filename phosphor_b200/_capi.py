@@ -129,8 +129,9 @@ class SceneSpec(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("trace_block", "emit_block", "gather_block", "trace_blocks_per_sm",
-                                          "emit_blocks_per_sm", "persistent", "nee_wavefront")] + \
-               [("reserved", C.c_uint32 * 5)]
+                                          "emit_blocks_per_sm", "persistent", "nee_wavefront",
+                                          "concurrent_passes")] + \
+               [("reserved", C.c_uint32 * 4)]
 
 
 SIZES = {Triangle: 176, Material: 96, UvTransformBlock: 192, Light: 128, CameraParams: 112, BvhNode: 32,
@@ -174,6 +175,7 @@ PROTOTYPES = [
     ("phx_get_stream", C.c_uint64, [VP]),
     ("phx_selftest_lookback_timeout", C.c_int, [C.c_int, C.c_uint32, C.POINTER(C.c_uint32)]),
     ("phx_scan_noalloc", C.c_int, [VP, VP, C.c_uint32, VP, C.c_uint64]),
+    ("phx_batch_set_active", C.c_int, [VP, C.c_uint32, C.c_int]),
     ("phx_set_materials", C.c_int, [VP, VP, C.c_uint32]),
     ("phx_set_lights", C.c_int, [VP, VP, C.c_uint32]),
     ("phx_adjoint_n_params", C.c_int, [VP, C.POINTER(C.c_uint32)]),

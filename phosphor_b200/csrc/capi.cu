@@ -281,6 +281,12 @@ PHX_API int phx_batch_iterate(void *b, uint32_t rounds, int mode) {
     });
 }
 
+PHX_API int phx_batch_set_active(void *b, uint32_t scene, int active) {
+    return guard([&]() -> int {
+        return b ? eng(b)->set_active(scene, active != 0) : fail(PHX_E_INVALID, "null batch");
+    });
+}
+
 PHX_API int phx_batch_read_buffer(void *b, uint32_t scene, int which, void *dst, uint64_t off, uint64_t bytes) {
     return guard([&]() -> int { return b ? eng(b)->read_buffer(scene, which, dst, off, bytes) : fail(PHX_E_INVALID, "null batch"); });
 }

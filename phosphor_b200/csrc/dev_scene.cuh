@@ -67,7 +67,7 @@ struct __align__(16) SceneDesc {
     u32 flags;
     u32 any_transmissive; // 0 -> shadow rays can stop at the first hit
     u32 nee_base;         // first deferred-NEE sample slot of this scene (pixel i, sample d at nee_base + i*ds + d)
-    u32 pad1;
+    u32 active;           // 0: a batch scene that has been retired; every stage skips it
 };
 
 // scene of global index gid: bases[s] <= gid < bases[s+1] (n+1 prefix offsets)
@@ -107,15 +107,28 @@ PHX_DI bool tri_test(const float4 *rec, float ox, float oy, float oz, float ow, 
     float a = ((r1.x * hx + r1.y * hy) + r1.z * hz) + 0.0f * 0.0f;
     if (fabsf(a) < EPS)
         return false;
-    float f = 1.0f / a;
     float sx = ox - r0.x, sy = oy - r0.y, sz = oz - r0.z, sw = ow - 0.0f;
-    float u = f * (((sx * hx + sy * hy) + sz * hz) + sw * 0.0f);
-    if (u < 0.0f || u > 1.0f)
+    const float un = ((sx * hx + sy * hy) + sz * hz) + sw * 0.0f;
+    // Division-free rejections, each implied by the exact test below (u = fl(un * fl(1/a)) carries
+    // a relative error below 2^-22): |un| > 1.0001|a| gives |u| > 1, so u > 1 or u < 0; a sign
+    // opposite to a's with |un| >= 2^-60|a| gives u < 0 (no underflow to -0).  NaNs fail every
+    // comparison and fall through to the exact test.
+    const float aa = fabsf(a), th = aa * 8.6736174e-19f; // 2^-60
+    if (fabsf(un) > aa * 1.0001f || ((un > 0.0f) != (a > 0.0f) && fabsf(un) >= th))
         return false;
     float qx = sy * r1.z - sz * r1.y;
     float qy = sz * r1.x - sx * r1.z;
     float qz = sx * r1.y - sy * r1.x;
-    float v = f * (((dx * qx + dy * qy) + dz * qz) + dw * 0.0f);
+    const float vn = ((dx * qx + dy * qy) + dz * qz) + dw * 0.0f;
+    // the same for v, and u + v > 1 when |un| + |vn| > 1.0001|a| with u, v >= 0
+    if (fabsf(vn) > aa * 1.0001f || ((vn > 0.0f) != (a > 0.0f) && fabsf(vn) >= th) ||
+        fabsf(un) + fabsf(vn) > aa * 1.0001f)
+        return false;
+    float f = 1.0f / a;
+    float u = f * un;
+    if (u < 0.0f || u > 1.0f)
+        return false;
+    float v = f * vn;
     if (v < 0.0f || u + v > 1.0f)
         return false;
     float t = f * (((r2.x * qx + r2.y * qy) + r2.z * qz) + 0.0f * 0.0f);

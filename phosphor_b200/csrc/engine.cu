@@ -70,6 +70,12 @@ Engine::~Engine() {
         b.release();
     if (h_pinned)
         cudaFreeHost(h_pinned);
+    if (fork_ev)
+        cudaEventDestroy(fork_ev);
+    if (join_ev)
+        cudaEventDestroy(join_ev);
+    if (st_side)
+        cudaStreamDestroy(st_side);
     if (st)
         cudaStreamDestroy(st);
 }
@@ -273,6 +279,7 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
         return fail(PHX_E_INVALID, "too many direct-lighting samples per round for 31-bit slot indices");
     total_nee += d.n_pixels * d.direct_samples;
     d.flags = p.flags;
+    d.active = 1;
     d.any_transmissive = 0;
     for (uint32_t m = 0; m < s.n_materials; m++)
         if (s.materials[m].transmission >= 1e-5f)
@@ -298,6 +305,9 @@ int Engine::create(const phx_scene *scenes, const phx_params *params, uint32_t n
     device = dev;
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&st_side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
     init_kernels(device);
     sc.resize(n);
     uint32_t pix = 0, emit = 0, cell = 0;
@@ -363,6 +373,7 @@ int Engine::create(const phx_scene *scenes, const phx_params *params, uint32_t n
     tune.emit_blocks_per_sm = 8;
     tune.persistent = 1;
     tune.nee_wavefront = 1;
+    tune.concurrent_passes = 0;
     for (uint32_t i = 0; i < n; i++)
         if (params[i].flags & PHX_F_SIMPLE_TRAVERSAL)
             tune.persistent = 0;
@@ -400,16 +411,16 @@ GridBufs Engine::gb() const {
     return g;
 }
 
-void Engine::ev(int stage, bool end) {
+void Engine::ev(int stage, bool end, cudaStream_t s) {
     if (!profiling)
         return;
     cudaEvent_t &e = events[2 * stage + (end ? 1 : 0)];
     if (!e)
         cudaEventCreate(&e);
     if (capturing)
-        cudaEventRecordWithFlags(e, st, cudaEventRecordExternal);
+        cudaEventRecordWithFlags(e, s ? s : st, cudaEventRecordExternal);
     else
-        cudaEventRecord(e, st);
+        cudaEventRecord(e, s ? s : st);
 }
 
 void Engine::enq_seeds() {
@@ -433,17 +444,19 @@ void Engine::enq_trace() {
     stage_state |= 1;
 }
 
-void Engine::enq_emit() {
-    ev(ST_EMIT, false);
+void Engine::enq_emit(cudaStream_t s) {
+    if (!s)
+        s = st;
+    ev(ST_EMIT, false, s);
     EmitOut o{slot_pos.as<float4>(), slot_pd.as<uint2>(), counts.as<u32>()};
     launch_emit(lc(), o, (int)tune.emit_block, (int)tune.persistent, (int)tune.emit_blocks_per_sm,
-                d_queue.as<u32>() + 1, st);
-    ev(ST_EMIT, true);
-    ev(ST_EMIT_SCAN, false);
+                d_queue.as<u32>() + 1, s);
+    ev(ST_EMIT, true, s);
+    ev(ST_EMIT_SCAN, false, s);
     launch_scan(counts.as<u32>(), offsets.as<u32>(), (u64)total_emit + 1, scan_scr.p, d_ntotal.as<u32>(),
-                d_err.as<u32>(), st);
-    launch_compact(lc(), gb(), st);
-    ev(ST_EMIT_SCAN, true);
+                d_err.as<u32>(), s);
+    launch_compact(lc(), gb(), s);
+    ev(ST_EMIT_SCAN, true, s);
     stage_state |= 2;
 }
 
@@ -576,7 +589,27 @@ int Engine::scene_photon_range(uint32_t s, uint32_t *off, uint32_t *n) {
     return PHX_OK;
 }
 
+bool Engine::any_active() const {
+    for (const auto &s : sc)
+        if (s.desc.active)
+            return true;
+    return false;
+}
+
+int Engine::set_active(uint32_t scene, bool on) {
+    if (scene >= sc.size())
+        return fail(PHX_E_INVALID, "scene index out of range");
+    if ((sc[scene].desc.active != 0) == on)
+        return PHX_OK;
+    adjoint_invalidate();
+    CK(cudaStreamSynchronize(st));
+    sc[scene].desc.active = on ? 1u : 0u;
+    return upload_descs();
+}
+
 int Engine::plain_round() {
+    if (!any_active())
+        return PHX_OK;
     enq_seeds();
     enq_trace();
     enq_emit();
@@ -589,7 +622,7 @@ int Engine::plain_round() {
         uint32_t off, n;
         if ((r = scene_photon_range(s, &off, &n)))
             return r;
-        if (n == 0)
+        if (n == 0 && sc[s].desc.active)
             return fail(PHX_E_NO_PHOTONS, "no photon hit (renderer.cpp:117-118)");
         sc[s].n_photons_last = n;
     }
@@ -599,10 +632,7 @@ int Engine::plain_round() {
     if (r)
         return r;
     accumulate_profile();
-    for (auto &s : sc) {
-        s.rounds++;
-        s.total_emitted += s.prm.photons_per_round;
-    }
+    count_round(1);
     return PHX_OK;
 }
 
@@ -613,8 +643,19 @@ int Engine::capture(bool with_seeds, cudaGraph_t *g, cudaGraphExec_t *ge) {
     capturing = true;
     if (with_seeds)
         enq_seeds();
-    enq_trace();
-    enq_emit();
+    if (tune.concurrent_passes) {
+        // the photon pass only shares the round seed with the camera pass: fork it onto a second
+        // branch of the graph and join before the hash stage
+        cudaEventRecord(fork_ev, st);
+        cudaStreamWaitEvent(st_side, fork_ev, 0);
+        enq_emit(st_side);
+        enq_trace();
+        cudaEventRecord(join_ev, st_side);
+        cudaStreamWaitEvent(st, join_ev, 0);
+    } else {
+        enq_trace();
+        enq_emit();
+    }
     enq_hash_sort();
     enq_gather();
     capturing = false;
@@ -629,6 +670,8 @@ int Engine::capture(bool with_seeds, cudaGraph_t *g, cudaGraphExec_t *ge) {
 
 void Engine::count_round(uint32_t rounds) {
     for (auto &s : sc) {
+        if (!s.desc.active)
+            continue;
         s.rounds += rounds;
         s.total_emitted += (uint64_t)rounds * s.prm.photons_per_round;
     }
@@ -636,6 +679,8 @@ void Engine::count_round(uint32_t rounds) {
 
 int Engine::graph_rounds(uint32_t rounds) {
     adjoint_invalidate();
+    if (!any_active())
+        return PHX_OK;
     int r;
     if (!gexec && (r = capture(true, &graph, &gexec)))
         return r;
@@ -661,6 +706,8 @@ int Engine::graph_rounds(uint32_t rounds) {
 
 int Engine::seeded_round(uint32_t seed) {
     adjoint_invalidate();
+    if (!any_active())
+        return PHX_OK;
     int r;
     if (!gexec_host && (r = capture(false, &graph_host, &gexec_host)))
         return r;

@@ -66,7 +66,7 @@ class Engine {
     // enqueue (no host sync)
     void enq_seeds();
     void enq_trace();
-    void enq_emit();
+    void enq_emit(cudaStream_t s = nullptr); // nullptr: the engine's stream
     void enq_hash_sort();
     void enq_gather();
     void enq_round();
@@ -87,6 +87,8 @@ class Engine {
     void set_profiling(bool on);
     void stage_ms(float *out) const;
     void invalidate_graph();
+    int set_active(uint32_t scene, bool on); // retire / resume a scene of a batch
+    bool any_active() const;
 
     // differentiation (single-scene engines; engine_adjoint.cu)
     int set_materials(const phx_material *m, uint32_t n);
@@ -114,7 +116,9 @@ class Engine {
     int upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, uint32_t *pix, uint32_t *emit,
                      uint32_t *cell, uint64_t *slot);
     int scene_photon_range(uint32_t s, uint32_t *off, uint32_t *n);
-    void ev(int stage, bool end);
+    void ev(int stage, bool end, cudaStream_t s = nullptr);
+    cudaStream_t st_side = nullptr;          // second branch of a captured round (photon pass)
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     void accumulate_profile();
 
     DevBuf d_desc, d_pix_bases, d_emit_bases, d_nee_bases, d_seeds, d_rng, d_err, d_ovf, d_queue, d_ntotal;

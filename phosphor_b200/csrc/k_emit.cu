@@ -80,6 +80,10 @@ __global__ void __launch_bounds__(128) k_emit(LaunchCtx lc, EmitOut out) {
         return;
     u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.emit_bases, lc.n_scenes, gid);
     const SceneDesc &sc = lc.scenes[s];
+    if (!sc.active) { // retired batch scene: no photons
+        out.counts[gid] = 0;
+        return;
+    }
     u32 ovf = 0;
     out.counts[gid] = emit_path(sc, __ldg(&lc.seeds[s]), gid - sc.emit_base, out, &ovf);
     if (ovf)
@@ -173,7 +177,7 @@ __global__ void __launch_bounds__(128) k_emit_persistent(LaunchCtx lc, EmitOut o
                     const SceneDesc *sc = lc.scenes + s;
                     pp_start(p, sc, __ldg(&lc.seeds[s]), gid - sc->emit_base, gid);
                     active = true;
-                    if (sc->max_bounces == 0) {
+                    if (sc->max_bounces == 0 || !sc->active) { // retired batch scene: no photons
                         out.counts[gid] = 0;
                         active = false;
                     }

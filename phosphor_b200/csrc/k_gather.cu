@@ -115,7 +115,8 @@ __global__ void __launch_bounds__(128) k_gather(LaunchCtx lc, GatherBufs g) {
     if (gid >= lc.total_pixels)
         return;
     u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gid);
-    gather_pixel(lc.scenes[s], gid, g);
+    if (lc.scenes[s].active)
+        gather_pixel(lc.scenes[s], gid, g);
 }
 
 void launch_gather(const LaunchCtx &lc, const GatherBufs &g, int block, cudaStream_t st) {

@@ -142,6 +142,8 @@ __global__ void __launch_bounds__(128) k_trace(LaunchCtx lc, TraceOut out) {
         return;
     u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gid);
     const SceneDesc &sc = lc.scenes[s];
+    if (!sc.active)
+        return;
     u32 ovf = 0;
     trace_pixel(sc, __ldg(&lc.seeds[s]), gid - sc.pixel_base, out, gid, &ovf, lc.nee_defer != 0);
     if (ovf)
@@ -413,14 +415,16 @@ __global__ void __launch_bounds__(128) k_trace_persistent(LaunchCtx lc, TraceOut
                 if (gid < lc.total_pixels) {
                     const u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gid);
                     const SceneDesc *sc = lc.scenes + s;
-                    cp_start(p, sc, __ldg(&lc.seeds[s]), gid - sc->pixel_base, gid);
-                    active = true;
+                    if (sc->active) { // a retired scene's pixel is skipped; the lane refills next step
+                        cp_start(p, sc, __ldg(&lc.seeds[s]), gid - sc->pixel_base, gid);
+                        active = true;
+                    }
                 } else {
                     exhausted = true;
                 }
             }
         }
-        if (!__any_sync(0xffffffffu, active))
+        if (!__any_sync(0xffffffffu, active || !exhausted))
             break;
         if (active) {
             Hit h;
@@ -442,6 +446,8 @@ __global__ void __launch_bounds__(128) k_shadow(LaunchCtx lc, TraceOut out) {
         return;
     const u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.nee_bases, lc.n_scenes, g);
     const SceneDesc &sc = lc.scenes[s];
+    if (!sc.active)
+        return;
     const u32 pixel = (g - sc.nee_base) / sc.direct_samples;
     const u32 gpix = sc.pixel_base + pixel;
     if (out.emission[gpix].w != 1.0f)
@@ -470,6 +476,8 @@ __global__ void __launch_bounds__(256) k_nee_resolve(LaunchCtx lc, TraceOut out)
         return;
     const u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gpix);
     const SceneDesc &sc = lc.scenes[s];
+    if (!sc.active)
+        return;
     const u32 ds = sc.direct_samples;
     const float4 *v = out.nee_val + sc.nee_base + (size_t)(gpix - sc.pixel_base) * ds;
     float4 sum = zero4();

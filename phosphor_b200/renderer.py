@@ -361,6 +361,10 @@ class Batch:
     def iterate(self, rounds: int, graph: bool = True) -> None:
         A.check(self._lib.phx_batch_iterate(self.h, rounds, 1 if graph else 0))
 
+    def set_active(self, s: int, active: bool) -> None:
+        """Retire (False) or resume a scene: retired scenes cost no work in later rounds."""
+        A.check(self._lib.phx_batch_set_active(self.h, s, int(active)))
+
     def info(self, s: int) -> A.Info:
         inf = A.Info()
         A.check(self._lib.phx_batch_get_info(self.h, s, C.byref(inf)))

@@ -160,6 +160,25 @@ def time_batched(specs, rounds: int, device: int = 0) -> float:
     return dt
 
 
+def time_batched_schedule(specs, r_star: list[int], device: int = 0) -> float:
+    """Wall seconds for the batch in the graph form to give every scene its own number of rounds:
+    rounds run for all active scenes, and each scene is retired as soon as it has had r_star[s]."""
+    b = Batch([s.scene() for s in specs], [s.args() for s in specs], device=device)
+    order = sorted(set(r_star))
+    done = 0
+    t0 = time.perf_counter()  # includes the graph capture of the first round
+    for target in order:
+        if target > done:
+            b.iterate(target - done, graph=True)
+            done = target
+        for i, r in enumerate(r_star):
+            if r == target:
+                b.set_active(i, False)
+    dt = time.perf_counter() - t0
+    b.close()
+    return dt
+
+
 def gpu_reference(spec: SceneSpec, rounds: int, seed_offset: int = 1000003, device: int = 0) -> np.ndarray:
     """Long fp32 render with an independent seed (calibration only; the FP64 oracle is the target)."""
     r = Renderer(spec.args(seed=spec.seed + seed_offset), device=device)

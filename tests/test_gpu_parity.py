@@ -299,6 +299,33 @@ def test_batch_equals_single_scenes():
     batch.close()
 
 
+def test_batch_retired_scene_stops_and_others_continue():
+    """A retired scene keeps its state and round count; the others go on exactly as alone."""
+    specs = [("cornell", dict(photons_per_round=1 << 13, seed=3)),
+             ("caustic", dict(photons_per_round=1 << 12, seed=4)),
+             ("atrium", dict(photons_per_round=1 << 12, seed=5))]
+    made = [make(n, **kw) for n, kw in specs]
+    batch = P.Batch([s for s, _ in made], [a for _, a in made])
+    batch.iterate(2, graph=True)
+    batch.set_active(1, False)
+    batch.iterate(3, graph=True)
+    assert [batch.info(i).rounds_done for i in range(3)] == [5, 2, 5]
+    for i, (scene, args) in enumerate(made):
+        with P.Renderer(args) as r:
+            r.set_scene(scene)
+            r.iterate(2 if i == 1 else 5)
+            for buf in ["FLUX", "PHOTON_WEIGHT", "RADIANCE"]:
+                assert np.array_equal(batch.read(i, buf).view(np.uint32), r.read(buf).view(np.uint32)), (i, buf)
+    batch.set_active(1, True)
+    batch.iterate(1, graph=True)
+    assert batch.info(1).rounds_done == 3
+    for i in range(3):
+        batch.set_active(i, False)
+    batch.iterate(2, graph=True)  # nothing active: no work, no error
+    assert [batch.info(i).rounds_done for i in range(3)] == [6, 3, 6]
+    batch.close()
+
+
 def test_image_formation_matches_output_cpp():
     scene, args = make("cornell")
     with P.Renderer(args) as r:
