@@ -215,6 +215,8 @@ def run_ours(a, cfg: dict) -> dict | None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
     args = make_args(cfg)
+    if a.binary_bvh:
+        args.flags = args.flags | 4  # PHX_F_BINARY_BVH
     scene = P.SceneData.generate(cfg["kind"], seed=1, width=args.width, height=args.height, detail=cfg["detail"])
     r = P.Renderer(args, device=local)
     r.set_scene(scene)
@@ -448,6 +450,7 @@ def main() -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--simple", action="store_true", help="one-thread-per-item kernels instead of lane refill")
     ap.add_argument("--persistent", action="store_true", help="lane-refill state-machine kernels")
+    ap.add_argument("--binary-bvh", action="store_true", help="traverse child pairs instead of 4-wide nodes")
     ap.add_argument("--concurrent-passes", action="store_true",
                     help="camera and photon passes on two branches of the captured round")
     ap.add_argument("--scale", type=int, default=1,

@@ -162,6 +162,7 @@ typedef struct phx_params {
 #define PHX_F_DEFAULT 0u
 #define PHX_F_SIMPLE_TRAVERSAL 1u /* one-thread-per-ray kernels instead of the persistent ones */
 #define PHX_F_REFERENCE_BVH 2u    /* traverse the reference's median-split tree instead of the SAH tree */
+#define PHX_F_BINARY_BVH 4u       /* traverse the SAH tree as child pairs instead of 4-wide nodes */
 
 /* Counters and sizes of a context. */
 typedef struct phx_info {

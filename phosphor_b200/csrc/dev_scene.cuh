@@ -26,7 +26,7 @@ namespace phx {
 
 struct __align__(16) SceneDesc {
     // geometry, device pointers
-    const float4 *cnodes;   // 4 float4 per inner node
+    const float4 *cnodes;   // inner nodes: 4 float4 per child pair, or 7 per 4-wide node
     const float4 *trirec;   // 3 float4 per triangle (leaf order)
     const float4 *tri_nrm;  // n0,n1,n2 per triangle (leaf order)
     const float4 *tri_tan;  // t0,t1,t2
@@ -62,7 +62,7 @@ struct __align__(16) SceneDesc {
     u32 pixel_base;       // first pixel of this scene
     u32 emit_base;        // first photon path of this scene
     u32 cell_base;        // first cell of this scene
-    u32 pad0;
+    u32 wide;             // 1: cnodes holds 4-wide nodes (7 float4 each), 0: child pairs (4 float4)
     u64 slot_base;        // first photon slot of this scene (slot j of path t at slot_base + j*n_emit + t)
     u32 flags;
     u32 any_transmissive; // 0 -> shadow rays can stop at the first hit
@@ -162,6 +162,28 @@ PHX_DI void box2(const float4 &a, const float4 &b, const float4 &c, float ix, fl
     *hr = rnear <= rfar;
 }
 
+// Slab test of one child of a 4-wide node; returns its entry distance, or +inf on a miss.
+PHX_DI float box1(float mnx, float mxx, float mny, float mxy, float mnz, float mxz, float ix, float iy, float iz,
+                  float oix, float oiy, float oiz, float t_min, float t_max) {
+    float x0 = __fmaf_rn(mnx, ix, -oix), x1 = __fmaf_rn(mxx, ix, -oix);
+    float y0 = __fmaf_rn(mny, iy, -oiy), y1 = __fmaf_rn(mxy, iy, -oiy);
+    float z0 = __fmaf_rn(mnz, iz, -oiz), z1 = __fmaf_rn(mxz, iz, -oiz);
+    float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), t_min));
+    float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), t_max));
+    return tn <= tf ? tn : __int_as_float(0x7f800000);
+}
+
+PHX_DI void sort2(float &ta, i32 &ra, float &tb, i32 &rb) {
+    if (tb < ta) {
+        float t = ta;
+        ta = tb;
+        tb = t;
+        i32 r = ra;
+        ra = rb;
+        rb = r;
+    }
+}
+
 // Closest hit in [t_min, t_max] (scene_intersect, hit.h:135-172).  Returns false on a miss.
 // `any` stops at the first accepted hit (only valid where the caller needs no specific hit).
 //
@@ -186,7 +208,53 @@ PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, floa
     while (__any_sync(mask, !done)) {
         if (done)
             continue;
-        if (node >= 0) { // inner node: test both children, descend into the nearer hit one
+        if (node >= 0 && sc.wide) { // 4-wide node: descend into the nearest hit child, stack the rest
+            const float4 *wn = sc.cnodes + 7 * (size_t)node;
+            const float4 mnx = __ldg(wn + 0), mxx = __ldg(wn + 1), mny = __ldg(wn + 2), mxy = __ldg(wn + 3);
+            const float4 mnz = __ldg(wn + 4), mxz = __ldg(wn + 5);
+            const int4 ch = __ldg(reinterpret_cast<const int4 *>(wn + 6));
+            // An empty slot (reference POP) never counts as hit: its box cannot be relied on to miss,
+            // since the slab test orders each pair of plane distances itself.
+            const float NOHIT = __int_as_float(0x7f800000);
+            float t0 = ch.x == POP ? NOHIT
+                                   : box1(mnx.x, mxx.x, mny.x, mxy.x, mnz.x, mxz.x, ix, iy, iz, oix, oiy, oiz, t_min,
+                                          closest);
+            float t1 = ch.y == POP ? NOHIT
+                                   : box1(mnx.y, mxx.y, mny.y, mxy.y, mnz.y, mxz.y, ix, iy, iz, oix, oiy, oiz, t_min,
+                                          closest);
+            float t2 = ch.z == POP ? NOHIT
+                                   : box1(mnx.z, mxx.z, mny.z, mxy.z, mnz.z, mxz.z, ix, iy, iz, oix, oiy, oiz, t_min,
+                                          closest);
+            float t3 = ch.w == POP ? NOHIT
+                                   : box1(mnx.w, mxx.w, mny.w, mxy.w, mnz.w, mxz.w, ix, iy, iz, oix, oiy, oiz, t_min,
+                                          closest);
+            i32 r0 = ch.x, r1 = ch.y, r2 = ch.z, r3 = ch.w;
+            sort2(t0, r0, t1, r1); // sorting network: ascending entry distance, misses (+inf) last
+            sort2(t2, r2, t3, r3);
+            sort2(t0, r0, t2, r2);
+            sort2(t1, r1, t3, r3);
+            sort2(t1, r1, t2, r2);
+            if (t0 == NOHIT) {
+                node = POP;
+            } else {
+                node = r0;
+                // the others, farthest first, so the nearest of them is popped first
+                const float ts[3] = {t3, t2, t1};
+                const i32 rs[3] = {r3, r2, r1};
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    if (ts[k] == NOHIT)
+                        continue;
+                    if (sp < TRAV_STACK) {
+                        stack_ref[sp] = rs[k];
+                        stack_t[sp] = ts[k];
+                        sp++;
+                    } else {
+                        *overflow += 1;
+                    }
+                }
+            }
+        } else if (node >= 0) { // child pair: test both children, descend into the nearer hit one
             const float4 *cn = sc.cnodes + 4 * (size_t)node;
             float4 a = __ldg(cn + 0), b = __ldg(cn + 1), c = __ldg(cn + 2);
             int4 ch = __ldg(reinterpret_cast<const int4 *>(cn + 3));

@@ -160,8 +160,15 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
     }
     if (!sah)
         bvh_pack(S.nodes, s.triangles, pk);
-    S.trav_depth = sah ? pk.depth : S.depth;
-    S.trav_inner = (uint32_t)(pk.cnodes.size() / 16);
+    // 4-wide nodes over the SAH tree (half the dependent node fetches per ray) unless asked for the
+    // binary form or the worst-case stack (3 pushes per level) could exceed the traversal stack
+    bool wide = false;
+    if (sah && !(p.flags & PHX_F_BINARY_BVH)) {
+        bvh_widen(pk);
+        wide = 3 * pk.wdepth + 4 < (uint32_t)TRAV_STACK;
+    }
+    S.trav_depth = wide ? pk.wdepth : sah ? pk.depth : S.depth;
+    S.trav_inner = wide ? (uint32_t)(pk.wnodes.size() / 28) : (uint32_t)(pk.cnodes.size() / 16);
     const uint32_t n = s.n_triangles;
     S.n_tris = n;
     std::vector<float> nrm((size_t)n * 12), tan((size_t)n * 12), uv((size_t)n * 8);
@@ -208,7 +215,8 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
     }
     S.bufs.resize(16);
     int r;
-    if ((r = upload(S.bufs[0], pk.cnodes.data(), pk.cnodes.size() * 4)) ||
+    const std::vector<float> &inner = wide ? pk.wnodes : pk.cnodes;
+    if ((r = upload(S.bufs[0], inner.data(), std::max<size_t>(inner.size(), 4) * 4)) ||
         (r = upload(S.bufs[1], pk.trirec.data(), pk.trirec.size() * 4)) ||
         (r = upload(S.bufs[2], nrm.data(), nrm.size() * 4)) || (r = upload(S.bufs[3], tan.data(), tan.size() * 4)) ||
         (r = upload(S.bufs[4], uv.data(), uv.size() * 4)) || (r = upload(S.bufs[5], ev.data(), ev.size() * 4)) ||
@@ -246,7 +254,8 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
     d.lights = S.bufs[13].as<phx_light>();
     d.lum_pref_sum = S.bufs[14].as<float>();
     d.envmap = S.bufs[15].as<float>();
-    d.root = pk.root;
+    d.root = wide ? pk.wroot : pk.root;
+    d.wide = wide ? 1u : 0u;
     d.n_tris = n;
     d.n_lights = s.n_lights;
     d.total_lum = s.n_lights ? lum[s.n_lights - 1] : 0.0f; // shading.cpp:26

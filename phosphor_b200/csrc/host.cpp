@@ -411,6 +411,78 @@ bool bvh_build_sah(const phx_triangle *tris, uint32_t n, const std::vector<uint3
     return next_tri == n;
 }
 
+void bvh_widen(PackedBvh &pk) {
+    struct Child {
+        float lo[3], hi[3];
+        int32_t ref;
+    };
+    auto pair = [&](int32_t node, Child *out) {
+        const float *c = &pk.cnodes[(size_t)node * 16];
+        int32_t refs[2];
+        std::memcpy(refs, &c[12], 8);
+        out[0] = {{c[0], c[2], c[8]}, {c[1], c[3], c[9]}, refs[0]};
+        out[1] = {{c[4], c[6], c[10]}, {c[5], c[7], c[11]}, refs[1]};
+    };
+    auto area = [](const Child &c) {
+        float x = c.hi[0] - c.lo[0], y = c.hi[1] - c.lo[1], z = c.hi[2] - c.lo[2];
+        return x * y + y * z + z * x;
+    };
+    pk.wnodes.clear();
+    pk.wdepth = 0;
+    pk.wroot = pk.root;
+    if (pk.root < 0)
+        return; // a single leaf
+    struct Item {
+        int32_t bin;
+        int32_t parent;
+        int slot;
+        uint32_t depth;
+    };
+    std::vector<Item> work{{pk.root, -1, 0, 0}};
+    while (!work.empty()) {
+        const Item it = work.back();
+        work.pop_back();
+        Child ch[4];
+        pair(it.bin, ch);
+        int n = 2;
+        while (n < 4) { // open the inner child with the largest surface
+            int best = -1;
+            float ba = -1.0f;
+            for (int k = 0; k < n; k++)
+                if (ch[k].ref >= 0 && area(ch[k]) > ba) {
+                    ba = area(ch[k]);
+                    best = k;
+                }
+            if (best < 0)
+                break;
+            Child two[2];
+            pair(ch[best].ref, two);
+            ch[best] = two[0];
+            ch[n++] = two[1];
+        }
+        const int32_t w = (int32_t)(pk.wnodes.size() / 28);
+        pk.wnodes.resize(pk.wnodes.size() + 28, 0.0f);
+        pk.wdepth = std::max(pk.wdepth, it.depth);
+        if (it.parent < 0)
+            pk.wroot = w;
+        else
+            std::memcpy(&pk.wnodes[(size_t)it.parent * 28 + 24 + it.slot], &w, 4);
+        float *o = &pk.wnodes[(size_t)w * 28];
+        for (int k = 0; k < 4; k++) {
+            const bool has = k < n;
+            for (int a = 0; a < 3; a++) {
+                o[8 * a + k] = has ? ch[k].lo[a] : 1e30f;
+                o[8 * a + 4 + k] = has ? ch[k].hi[a] : -1e30f;
+            }
+            const int32_t ref = has ? ch[k].ref : 0x7fffffff;
+            std::memcpy(&o[24 + k], &ref, 4);
+        }
+        for (int k = n - 1; k >= 0; k--) // pre-order: the first child is laid out next
+            if (ch[k].ref >= 0)
+                work.push_back({ch[k].ref, w, k, it.depth + 1});
+    }
+}
+
 // build_photon_hash_info (photon_hash.h:41-50)
 phx_photon_hash_data hash_info(const phx_bvh_node &root, uint32_t g) {
     phx_photon_hash_data d{};

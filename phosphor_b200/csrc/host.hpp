@@ -17,6 +17,9 @@ bool bvh_build(const phx_triangle *tris, uint32_t n, std::vector<phx_bvh_node> &
 // Device packing of a traversal BVH (see dev_scene.cuh).
 struct PackedBvh {
     std::vector<float> cnodes;      // 16 floats per inner node (child pair)
+    std::vector<float> wnodes;      // 28 floats per 4-wide node (bvh_widen)
+    int32_t wroot = 0;
+    uint32_t wdepth = 0;
     std::vector<float> trirec;      // 12 floats per triangle, device (leaf) order
     std::vector<uint32_t> leaf_tri; // device triangle index -> original triangle index
     int32_t root = 0;
@@ -32,6 +35,12 @@ void bvh_pack(const std::vector<phx_bvh_node> &nodes, const phx_triangle *tris, 
 // max_leaf triangles; triangle records carry the reference leaf rank for tie-breaking.
 bool bvh_build_sah(const phx_triangle *tris, uint32_t n, const std::vector<uint32_t> &ref_rank, uint32_t max_leaf,
                    PackedBvh &out);
+
+// Collapses the child-pair tree into 4-wide nodes (each node pulls up the grandchildren of its
+// largest inner children until it has 4): 7 float4 per node, SoA {minx[4], maxx[4], miny[4],
+// maxy[4], minz[4], maxz[4], refs[4]}; an empty slot has reference 0x7fffffff (which traversal
+// checks: its inverted box would not by itself make the slab test miss).
+void bvh_widen(PackedBvh &pk);
 
 phx_photon_hash_data hash_info(const phx_bvh_node &root, uint32_t grid_res);
 void scene_sphere(const phx_bvh_node &root, phx_f4 *center, float *radius);

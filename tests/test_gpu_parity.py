@@ -246,10 +246,12 @@ def test_kernel_forms_agree(name):
 @pytest.mark.parametrize("name", list(SCENES))
 def test_traversal_tree_does_not_change_results(name):
     """Traversing the reference median-split tree or binned-SAH trees with 1, 4 or 8 triangles per
-    leaf gives identical bits: closest hit, ties broken by the reference leaf rank."""
+    leaf, as 4-wide nodes or as child pairs, gives identical bits: closest hit, ties broken by the
+    reference leaf rank."""
     scene, args = make(name)
     variants = [dict(flags=A.PHX_F_REFERENCE_BVH), dict(bvh_leaf_size=1), dict(bvh_leaf_size=4),
-                dict(bvh_leaf_size=8)]
+                dict(bvh_leaf_size=8), dict(flags=A.PHX_F_BINARY_BVH),
+                dict(flags=A.PHX_F_BINARY_BVH, bvh_leaf_size=1)]
     outs = []
     for v in variants:
         a2 = make(name, **v)[1]
