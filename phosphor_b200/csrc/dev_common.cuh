@@ -22,6 +22,34 @@ typedef uint8_t u8;
 typedef uint64_t u64;
 
 #define PHX_DI __device__ __forceinline__
+// Large shading routines, by group: compiled out of line (one shared copy, a smaller instruction
+// footprint for the state-machine kernels) or inlined.
+#define PHX_OUTLINED static __device__ __noinline__
+#ifdef PHX_OUTLINE_NEE
+#define PHX_SHADE_NEE PHX_OUTLINED
+#else
+#define PHX_SHADE_NEE PHX_DI
+#endif
+#ifdef PHX_OUTLINE_BSDF
+#define PHX_SHADE_BSDF PHX_OUTLINED
+#else
+#define PHX_SHADE_BSDF PHX_DI
+#endif
+#ifdef PHX_OUTLINE_HIT
+#define PHX_SHADE_HIT PHX_OUTLINED
+#else
+#define PHX_SHADE_HIT PHX_DI
+#endif
+#ifdef PHX_OUTLINE_TEX
+#define PHX_SHADE_TEX PHX_OUTLINED
+#else
+#define PHX_SHADE_TEX PHX_DI
+#endif
+#ifdef PHX_OUTLINE_LIGHT
+#define PHX_SHADE_LIGHT PHX_OUTLINED
+#else
+#define PHX_SHADE_LIGHT PHX_DI
+#endif
 #define PHX_HDI __host__ __device__ __forceinline__
 
 // include/common/constants.h:6-45

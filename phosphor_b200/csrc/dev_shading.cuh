@@ -21,7 +21,7 @@ struct SurfaceHit {
 PHX_DI u32 tri_mat(const SceneDesc &sc, i32 tri) { return __float_as_uint(__ldg(&sc.trirec[3 * (size_t)tri].w)); }
 
 // hit.h:174-197 (compute_bary hit.h:31-43)
-PHX_DI SurfaceHit process_hit(const SceneDesc &sc, const Hit &h, float4 origin, float4 dir) {
+PHX_SHADE_HIT SurfaceHit process_hit(const SceneDesc &sc, const Hit &h, float4 origin, float4 dir) {
     SurfaceHit s;
     s.t = h.t;
     s.tri = h.tri;
@@ -102,7 +102,7 @@ PHX_DI float4 sample_texture(const SceneDesc &sc, u32 index, float ux, float uy)
     return w11 * Q11 + w12 * Q12 + w21 * Q21 + w22 * Q22;
 }
 
-PHX_DI float4 sample_texture_uv(const SceneDesc &sc, u32 mat_index, u32 tex_index, float ux, float uy, u32 slot) {
+PHX_SHADE_TEX float4 sample_texture_uv(const SceneDesc &sc, u32 mat_index, u32 tex_index, float ux, float uy, u32 slot) {
     const phx_uv_transform *t = &sc.uvt[mat_index].diff + slot;
     float sx = ux * t->uv_scale.x, sy = uy * t->uv_scale.y;
     float c = pm_cosf(t->uv_rotation), s = pm_sinf(t->uv_rotation);
@@ -149,7 +149,7 @@ PHX_DI float4 apply_normal_map(float4 ms, float4 gn, float4 t, float4 b) {
     return (len > EPS) ? (p / len) : gn;
 }
 
-PHX_DI ShadingContext evaluate_material(const SceneDesc &sc, const phx_material &mat, u32 mi, float ux, float uy,
+PHX_SHADE_HIT ShadingContext evaluate_material(const SceneDesc &sc, const phx_material &mat, u32 mi, float ux, float uy,
                                         float4 gn, float4 t, float4 b) {
     ShadingContext ctx;
     ctx.base_color = f4(mat.base_color);
@@ -278,7 +278,7 @@ struct BsdfSample {
 };
 
 // shading.h:150-213
-PHX_DI BsdfSample sample_bsdf(Rng *rng, const ShadingContext &ctx, float4 sn, float4 gn, float4 view, IorStack *ior,
+PHX_SHADE_BSDF BsdfSample sample_bsdf(Rng *rng, const ShadingContext &ctx, float4 sn, float4 gn, float4 view, IorStack *ior,
                               bool front) {
     BsdfSample s;
     float4 h = ggx_sample_vndf(rng, sn, gn, view, ctx.roughness);
@@ -424,7 +424,7 @@ PHX_DI u32 select_light(Rng *rng, const SceneDesc &sc, float *scale) {
 }
 
 // light_sampling.h:200-227
-PHX_DI void sample_light(Rng *rng, const SceneDesc &sc, float4 *origin, float4 *dir, float4 *power) {
+PHX_SHADE_LIGHT void sample_light(Rng *rng, const SceneDesc &sc, float4 *origin, float4 *dir, float4 *power) {
     if (sc.n_lights == 0 || sc.total_lum < EPS) {
         *origin = zero4();
         *dir = f4(0.0f, 1.0f, 0.0f, 0.0f);
@@ -479,7 +479,7 @@ PHX_DI void sample_light(Rng *rng, const SceneDesc &sc, float4 *origin, float4 *
 }
 
 // light_sampling.h:231-300
-PHX_DI bool sample_light_fragment(Rng *rng, const SceneDesc &sc, float4 pos, float4 normal, LightFragment *out) {
+PHX_SHADE_NEE bool sample_light_fragment(Rng *rng, const SceneDesc &sc, float4 pos, float4 normal, LightFragment *out) {
     if (sc.n_lights == 0 || sc.total_lum < EPS)
         return false;
     float scale;

@@ -14,6 +14,15 @@
 //    split at the ray queries.
 // Pixel i of a scene uses pcg_seed(round_seed + i), so results do not depend on which lane or
 // block traces it.
+//
+// This file compiles the light sampling of NEE, the texture lookups and the BSDF sampler out of
+// line: the camera-path kernels call them from several places, and one shared copy keeps their
+// instruction footprint small (measured: warps stalled on instruction fetch dominated, and the
+// persistent camera kernel ran 18 % faster out of line).  The photon kernels (k_emit.cu) measure
+// faster with everything inlined and keep it so.
+#define PHX_OUTLINE_NEE
+#define PHX_OUTLINE_TEX
+#define PHX_OUTLINE_BSDF
 #include "dev_shading.cuh"
 #include "kernels.hpp"
 
@@ -36,7 +45,7 @@ PHX_DI void write_result(const TraceOut &out, u32 gpix, const TraceResult &r) {
 // and its RNG draws (light choice, light point) never depend on the shadow rays' outcome, so the
 // loop is split: here the samples are drawn in order and each shadow ray is recorded; the shadow
 // wavefront traces them; the resolve kernel sums the contributions in sample order.
-PHX_DI void record_nee(const SceneDesc &sc, Rng *rng, float4 pos, float4 sn, float4 base, const TraceOut &out,
+PHX_SHADE_NEE void record_nee(const SceneDesc &sc, Rng *rng, float4 pos, float4 sn, float4 base, const TraceOut &out,
                        u32 slot) {
     for (u32 d = 0; d < sc.direct_samples; d++, slot++) {
         LightFragment f;
