@@ -227,6 +227,10 @@ def run_ours(a, cfg: dict) -> dict | None:
         if a.concurrent_passes:
             t.concurrent_passes = 1
         r.set_tuning(t)
+    tuned = None
+    if a.autotune:
+        tt = r.autotune(4)
+        tuned = {f: getattr(tt, f) for f, _ in tt._fields_ if f != "reserved"}
     ext = torch.cuda.ExternalStream(r.stream(), device=local)
     r.iterate(max(3, a.warmup))
 
@@ -329,7 +333,7 @@ def run_ours(a, cfg: dict) -> dict | None:
             "config": {"workload": a.config, "desc": cfg["desc"], "form": "CUDA-graph replay, all stages on device",
                        "l2": "per-iteration working set (~0.4 GB) larger than L2; scene geometry L2-resident",
                        "parallelism": f"replicas x{world}", "stored_photons": n_s, "pixels": Pn,
-                       "cells": C},
+                       "cells": C, "autotuned": tuned},
             "roofline": roofline, "rays": rays, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": kernels * a.steps, "kernels_per_round": kernels, "clocks": clk.summary()}
 
@@ -451,6 +455,7 @@ def main() -> int:
     ap.add_argument("--simple", action="store_true", help="one-thread-per-item kernels instead of lane refill")
     ap.add_argument("--persistent", action="store_true", help="lane-refill state-machine kernels")
     ap.add_argument("--binary-bvh", action="store_true", help="traverse child pairs instead of 4-wide nodes")
+    ap.add_argument("--autotune", action="store_true", help="run the library autotuner before timing")
     ap.add_argument("--concurrent-passes", action="store_true",
                     help="camera and photon passes on two branches of the captured round")
     ap.add_argument("--scale", type=int, default=1,

@@ -322,6 +322,13 @@ typedef struct phx_tuning {
 } phx_tuning;
 PHX_API int phx_get_tuning(void *ctx, phx_tuning *out);
 PHX_API int phx_set_tuning(void *ctx, const phx_tuning *in);
+/* Autotuner (no counterpart in the reference): times graph-replayed rounds of this context or batch
+ * under candidate tunings — lane refill on/off, NEE wavefront on/off, persistent grid sizes of the
+ * camera and photon kernels, concurrent passes on/off — by coordinate descent, keeps the fastest
+ * and writes it to *chosen (may be NULL).  Every candidate gives bit-identical results; the SPPM
+ * state, seeds and round counters are restored afterwards.  Each trial renders rounds_per_trial + 1
+ * rounds (1..64). */
+PHX_API int phx_autotune(void *ctx, uint32_t rounds_per_trial, phx_tuning *chosen);
 
 /* ---- measurement ------------------------------------------------------------------------------ */
 /* Records CUDA events around every stage of every later round (in graph replays too) and keeps

@@ -170,6 +170,7 @@ PROTOTYPES = [
     ("phx_batch_image", C.c_int, [VP, C.c_uint32, C.c_float, C.c_int, VP]),
     ("phx_get_tuning", C.c_int, [VP, C.POINTER(Tuning)]),
     ("phx_set_tuning", C.c_int, [VP, C.POINTER(Tuning)]),
+    ("phx_autotune", C.c_int, [VP, C.c_uint32, C.POINTER(Tuning)]),
     ("phx_profile", C.c_int, [VP, C.c_int]),
     ("phx_stage_ms", C.c_int, [VP, C.POINTER(C.c_float), C.c_uint32]),
     ("phx_get_stream", C.c_uint64, [VP]),

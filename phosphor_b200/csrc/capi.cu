@@ -325,6 +325,12 @@ PHX_API int phx_set_tuning(void *ctx, const phx_tuning *in) {
     });
 }
 
+PHX_API int phx_autotune(void *ctx, uint32_t rounds_per_trial, phx_tuning *chosen) {
+    return guard([&]() -> int {
+        return ctx ? eng(ctx)->autotune(rounds_per_trial, chosen) : fail(PHX_E_INVALID, "null context");
+    });
+}
+
 PHX_API int phx_profile(void *ctx, int enable) {
     return guard([&]() -> int {
         if (!ctx)

@@ -745,6 +745,101 @@ int Engine::upload_descs() {
     return PHX_OK;
 }
 
+int Engine::autotune(uint32_t rounds, phx_tuning *chosen) {
+    if (!any_active())
+        return fail(PHX_E_STATE, "no active scene to tune on");
+    if (rounds == 0 || rounds > 64)
+        return fail(PHX_E_INVALID, "rounds_per_trial must be 1..64");
+    adjoint_invalidate();
+    CK(cudaStreamSynchronize(st));
+    // the trials render real rounds: keep the state they overwrite
+    const size_t P = total_pixels, ns = sc.size();
+    DevBuf keep;
+    int r;
+    if ((r = keep.alloc(36 * P + 4 * ns)))
+        return r;
+    char *k = keep.as<char>();
+    CK(cudaMemcpy(k, flux.p, 16 * P, cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpy(k + 16 * P, radiance.p, 16 * P, cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpy(k + 32 * P, weight.p, 4 * P, cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpy(k + 36 * P, d_rng.p, 4 * ns, cudaMemcpyDeviceToDevice));
+    std::vector<SceneSlot> counters(ns);
+    for (size_t i = 0; i < ns; i++) {
+        counters[i].rounds = sc[i].rounds;
+        counters[i].total_emitted = sc[i].total_emitted;
+        counters[i].n_photons_last = sc[i].n_photons_last;
+    }
+    const int kept_state = stage_state;
+    const bool was_profiling = profiling;
+    if (was_profiling)
+        set_profiling(false);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto trial = [&](const phx_tuning &tt, float *ms) -> int {
+        tune = tt;
+        invalidate_graph();
+        int rr = graph_rounds(1); // capture + warm-up
+        if (rr)
+            return rr;
+        if (cudaEventRecord(e0, st) != cudaSuccess)
+            return fail(PHX_E_CUDA, "event record failed");
+        if ((rr = graph_rounds(rounds)))
+            return rr;
+        if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(ms, e0, e1) != cudaSuccess)
+            return fail(PHX_E_CUDA, "event timing failed");
+        return PHX_OK;
+    };
+    phx_tuning best = tune;
+    float best_ms = 0.0f;
+    r = trial(best, &best_ms);
+    // coordinate descent over the knobs that leave every result bit-identical
+    auto knob = [&](uint32_t phx_tuning::*f, std::initializer_list<uint32_t> values) {
+        for (uint32_t v : values) {
+            if (r || best.*f == v)
+                continue;
+            phx_tuning c = best;
+            c.*f = v;
+            float ms = 0.0f;
+            r = trial(c, &ms);
+            if (!r && ms < best_ms) {
+                best_ms = ms;
+                best = c;
+            }
+        }
+    };
+    knob(&phx_tuning::persistent, {1u, 0u});
+    knob(&phx_tuning::nee_wavefront, {1u, 0u});
+    if (best.persistent) {
+        knob(&phx_tuning::trace_blocks_per_sm, {2u, 4u, 6u, 8u, 12u, 16u});
+        knob(&phx_tuning::emit_blocks_per_sm, {2u, 4u, 6u, 8u, 12u, 16u});
+    }
+    knob(&phx_tuning::concurrent_passes, {0u, 1u});
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    tune = best;
+    invalidate_graph();
+    // restore the state
+    CK(cudaMemcpy(flux.p, k, 16 * P, cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpy(radiance.p, k + 16 * P, 16 * P, cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpy(weight.p, k + 32 * P, 4 * P, cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpy(d_rng.p, k + 36 * P, 4 * ns, cudaMemcpyDeviceToDevice));
+    for (size_t i = 0; i < ns; i++) {
+        sc[i].rounds = counters[i].rounds;
+        sc[i].total_emitted = counters[i].total_emitted;
+        sc[i].n_photons_last = counters[i].n_photons_last;
+    }
+    stage_state = kept_state;
+    if (was_profiling)
+        set_profiling(true);
+    if (r)
+        return r;
+    if (chosen)
+        *chosen = best;
+    return PHX_OK;
+}
+
 int Engine::set_alpha(float alpha) {
     adjoint_invalidate();
     CK(cudaStreamSynchronize(st));

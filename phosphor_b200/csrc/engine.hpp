@@ -88,6 +88,9 @@ class Engine {
     void stage_ms(float *out) const;
     void invalidate_graph();
     int set_active(uint32_t scene, bool on); // retire / resume a scene of a batch
+    // Picks the launch tuning that minimises the time of a graph-replayed round (coordinate descent
+    // over the result-neutral knobs); the SPPM state is saved and restored around the trials.
+    int autotune(uint32_t rounds_per_trial, phx_tuning *chosen);
     bool any_active() const;
 
     // differentiation (single-scene engines; engine_adjoint.cu)

@@ -290,6 +290,13 @@ class Renderer:
     def profile(self, on: bool) -> None:
         A.check(self._lib.phx_profile(self._need(), int(on)))
 
+    def autotune(self, rounds_per_trial: int = 4) -> A.Tuning:
+        """Times candidate launch tunings on graph-replayed rounds, keeps the fastest (results are
+        bit-identical under all of them; the render state is restored)."""
+        t = A.Tuning()
+        A.check(self._lib.phx_autotune(self._need(), rounds_per_trial, C.byref(t)))
+        return t
+
     def stage_ms(self) -> dict[str, float]:
         out = (C.c_float * len(A.STAGES))()
         A.check(self._lib.phx_stage_ms(self._need(), out, len(A.STAGES)))
@@ -393,6 +400,12 @@ class Batch:
 
     def profile(self, on: bool) -> None:
         A.check(self._lib.phx_profile(self.h, int(on)))
+
+    def autotune(self, rounds_per_trial: int = 4) -> A.Tuning:
+        """phx_autotune over the whole batch (every stage launches all scenes at once)."""
+        t = A.Tuning()
+        A.check(self._lib.phx_autotune(self.h, rounds_per_trial, C.byref(t)))
+        return t
 
     def stage_ms(self) -> dict[str, float]:
         out = (C.c_float * len(A.STAGES))()

@@ -328,6 +328,27 @@ def test_batch_retired_scene_stops_and_others_continue():
     batch.close()
 
 
+def test_autotune_keeps_state_and_results():
+    """The autotuner renders trial rounds but restores state, seeds and counters, and the tuning it
+    picks gives the same bits as the default one."""
+    scene, args = make("caustic")
+    with P.Renderer(args) as a, P.Renderer(args) as b:
+        a.set_scene(scene)
+        b.set_scene(scene)
+        a.iterate(2)
+        b.iterate(2)
+        before = {k: a.read(k).view(np.uint32).copy() for k in ["FLUX", "PHOTON_WEIGHT", "RADIANCE"]}
+        t = a.autotune(2)
+        assert t.persistent in (0, 1) and t.nee_wavefront in (0, 1)
+        assert a.info().rounds_done == 2 and a.info().total_photons_emitted == b.info().total_photons_emitted
+        for k, v in before.items():
+            assert np.array_equal(a.read(k).view(np.uint32), v), k
+        a.iterate(3)
+        b.iterate(3)
+        for k in ["FLUX", "PHOTON_WEIGHT", "RADIANCE"]:
+            assert np.array_equal(a.read(k).view(np.uint32), b.read(k).view(np.uint32)), k
+
+
 def test_image_formation_matches_output_cpp():
     scene, args = make("cornell")
     with P.Renderer(args) as r:
