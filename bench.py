@@ -19,7 +19,9 @@ roofline = the dominant kernel's algorithmic bytes per launch / its CUDA-event d
            the measured HBM copy bandwidth.
 --impl reference times the reference algorithm on the host cores (the oracle port: the
 reference's OpenCL kernels have no CPU runtime here) on a bounded sample of the same workload.
-Multi-GPU: N ranks render independent replicas (weak scaling, no collective on this path).
+Multi-GPU: N ranks render independent replicas (weak scaling, no collective on this path); with
+--shard they render one image together (strong scaling): pixel and photon-path ranges per rank and
+one NCCL all-gather of the stored photons per round, results bit-identical to one GPU.
 """
 from __future__ import annotations
 
@@ -423,6 +425,75 @@ def time_to_rmse(a) -> dict | None:
     return out
 
 
+def run_shard(a, cfg: dict) -> dict | None:
+    """One image over N GPUs (strong scaling): rank r traces its pixel range and emits its range of
+    photon paths; one NCCL all-gather of the stored photons per round; every rank gathers its own
+    pixels (bit-identical to one GPU).  Rounds are host-synchronised (the exchange needs the
+    per-rank photon counts)."""
+    import datetime
+
+    import torch
+
+    import phosphor_b200 as P
+    from phosphor_b200.renderer import nccl_unique_id
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    args = make_args(cfg)
+    scene = P.SceneData.generate(cfg["kind"], seed=1, width=args.width, height=args.height, detail=cfg["detail"])
+    r = P.Renderer(args, device=local)
+    r.set_scene(scene)
+    r.shard(rank, world)
+    uid = [nccl_unique_id() if rank == 0 else None]
+    if dist is not None:
+        dist.broadcast_object_list(uid, src=0)
+    r.shard_nccl(uid[0])
+    ext = torch.cuda.ExternalStream(r.stream(), device=local)
+    for _ in range(max(3, a.warmup)):
+        r.shard_round()
+
+    def barrier():
+        torch.cuda.synchronize(local)
+        if dist is not None:
+            dist.barrier()
+
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(ext)
+        for _ in range(a.steps):
+            r.shard_round()
+        ev1.record(ext)
+        ev1.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        tt = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    info = r.info()
+    r.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    value = args.photons_per_round * a.steps / (ms / 1e3) / 1e6
+    return {"metric": METRIC, "value": round(value, 3), "unit": METRIC, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": a.config, "desc": cfg["desc"], "form": "sharded rounds, host-synchronised",
+                       "parallelism": f"pixel and photon-path shards x{world}, one NCCL photon all-gather per round",
+                       "stored_photons": info.n_photons},
+            "e2e": {"value": round(value, 3), "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 8 + 4 * world},
+            "gpu_launches": info.kernels_per_round * a.steps, "clocks": clk.summary()}
+
+
 def run_inverse(a) -> dict:
     """Differentiable SPPM: recover 32 materials' base colour and roughness and the sun's power of
     the atrium at 512x512 from target images, Adam 200 steps at lr 1e-2, 2^20 photons per forward
@@ -456,6 +527,8 @@ def main() -> int:
     ap.add_argument("--persistent", action="store_true", help="lane-refill state-machine kernels")
     ap.add_argument("--binary-bvh", action="store_true", help="traverse child pairs instead of 4-wide nodes")
     ap.add_argument("--autotune", action="store_true", help="run the library autotuner before timing")
+    ap.add_argument("--shard", action="store_true",
+                    help="one image over all GPUs (strong scaling) instead of one replica per GPU")
     ap.add_argument("--concurrent-passes", action="store_true",
                     help="camera and photon passes on two branches of the captured round")
     ap.add_argument("--scale", type=int, default=1,
@@ -486,7 +559,7 @@ def main() -> int:
             return 0
         print(json.dumps(run_reference(a, cfg)))
         return 0
-    out = run_ours(a, cfg)
+    out = run_shard(a, cfg) if a.shard else run_ours(a, cfg)
     if out is not None:
         if not a.no_rmse and out["n_gpus"] == 1 and a.scale == 1:
             out["time_to_rmse"] = time_to_rmse(a)

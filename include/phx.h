@@ -341,6 +341,31 @@ PHX_API int phx_stage_ms(void *ctx, float *out, uint32_t n);
 /* The CUDA stream (cudaStream_t) every stage of the context or batch is enqueued on. */
 PHX_API uint64_t phx_get_stream(void *ctx);
 
+/* ---- one image over several GPUs (single-scene contexts) -------------------------------------------
+ * No counterpart in the reference (single device).  Each process creates a context for the same
+ * scene and params on its own GPU and calls phx_shard(ctx, rank, world): rank r traces the pixel
+ * range [P*r/W, P*(r+1)/W) and emits the photon paths [E*r/W, E*(r+1)/W).  In each round the ranks
+ * exchange their stored photons once; concatenated in rank order they are the global canonical
+ * photons, so every rank hashes, sorts and gathers exactly what a single GPU would, and each pixel's
+ * flux, weight and radiance are bit-identical to a single-GPU render (pixels outside a rank's range
+ * stay zero there).  A sharded context renders only through these calls (phx_round, phx_iterate and
+ * phx_round_seeded return PHX_E_STATE).
+ *   NCCL transport: rank 0 calls phx_nccl_unique_id, the id reaches every rank by any host channel,
+ *   every rank calls phx_shard_nccl (collective), then phx_shard_round per round.  NCCL is loaded at
+ *   run time (the process's own libnccl.so.2 if one is loaded); PHX_E_UNSUPPORTED without it.
+ *   Host transport: phx_shard_begin (seed, camera pass, photon pass; *n_local = photons stored by this
+ *   rank), phx_shard_get_photons (this rank's photons: float4 positions, uint32 pairs of RGBE power and
+ *   octahedral direction), the caller concatenates all ranks' photons in rank order and hands them to
+ *   every rank with phx_shard_put_photons, then phx_shard_end (hash, sort, gather). */
+PHX_API int phx_shard(void *ctx, uint32_t rank, uint32_t world);
+PHX_API int phx_shard_begin(void *ctx, uint32_t *n_local);
+PHX_API int phx_shard_get_photons(void *ctx, float *pos4, uint32_t *pd2, uint32_t n);
+PHX_API int phx_shard_put_photons(void *ctx, const float *pos4, const uint32_t *pd2, uint32_t n_all);
+PHX_API int phx_shard_end(void *ctx);
+PHX_API int phx_nccl_unique_id(uint8_t *out, uint32_t n);
+PHX_API int phx_shard_nccl(void *ctx, const uint8_t *id);
+PHX_API int phx_shard_round(void *ctx);
+
 /* ---- differentiation (single-scene contexts) -------------------------------------------------------
  * No counterpart in the reference.  Parameters θ: per material its base colour (r, g, b) and
  * roughness, per light its power (r, g, b); gradients are laid out as 4 floats per material

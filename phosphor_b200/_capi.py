@@ -177,6 +177,14 @@ PROTOTYPES = [
     ("phx_selftest_lookback_timeout", C.c_int, [C.c_int, C.c_uint32, C.POINTER(C.c_uint32)]),
     ("phx_scan_noalloc", C.c_int, [VP, VP, C.c_uint32, VP, C.c_uint64]),
     ("phx_batch_set_active", C.c_int, [VP, C.c_uint32, C.c_int]),
+    ("phx_shard", C.c_int, [VP, C.c_uint32, C.c_uint32]),
+    ("phx_shard_begin", C.c_int, [VP, C.POINTER(C.c_uint32)]),
+    ("phx_shard_get_photons", C.c_int, [VP, VP, VP, C.c_uint32]),
+    ("phx_shard_put_photons", C.c_int, [VP, VP, VP, C.c_uint32]),
+    ("phx_shard_end", C.c_int, [VP]),
+    ("phx_nccl_unique_id", C.c_int, [VP, C.c_uint32]),
+    ("phx_shard_nccl", C.c_int, [VP, VP]),
+    ("phx_shard_round", C.c_int, [VP]),
     ("phx_set_materials", C.c_int, [VP, VP, C.c_uint32]),
     ("phx_set_lights", C.c_int, [VP, VP, C.c_uint32]),
     ("phx_adjoint_n_params", C.c_int, [VP, C.POINTER(C.c_uint32)]),

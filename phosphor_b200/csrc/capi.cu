@@ -2,6 +2,7 @@
 // validates its handle and arguments, catches every C++ exception and reports failures as status
 // codes with a message in phx_last_error(); nothing traps or throws across the boundary.
 #include "engine.hpp"
+#include "nccl_dl.hpp"
 
 #include <cstring>
 #include <new>
@@ -396,6 +397,55 @@ PHX_API int phx_adjoint_backward(void *ctx, const float *dl_dimage, float *grad,
     return guard([&]() -> int {
         return ctx ? eng(ctx)->adjoint_backward(dl_dimage, grad, n_grad) : fail(PHX_E_INVALID, "null context");
     });
+}
+
+PHX_API int phx_shard(void *ctx, uint32_t rank, uint32_t world) {
+    return guard([&]() -> int { return ctx ? eng(ctx)->set_shard(rank, world) : fail(PHX_E_INVALID, "null context"); });
+}
+
+PHX_API int phx_shard_begin(void *ctx, uint32_t *n_local) {
+    return guard([&]() -> int { return ctx ? eng(ctx)->shard_begin(n_local) : fail(PHX_E_INVALID, "null context"); });
+}
+
+PHX_API int phx_shard_get_photons(void *ctx, float *pos4, uint32_t *pd2, uint32_t n) {
+    return guard([&]() -> int {
+        return ctx ? eng(ctx)->shard_get_photons(pos4, pd2, n) : fail(PHX_E_INVALID, "null context");
+    });
+}
+
+PHX_API int phx_shard_put_photons(void *ctx, const float *pos4, const uint32_t *pd2, uint32_t n_all) {
+    return guard([&]() -> int {
+        return ctx ? eng(ctx)->shard_put_photons(pos4, pd2, n_all) : fail(PHX_E_INVALID, "null context");
+    });
+}
+
+PHX_API int phx_shard_end(void *ctx) {
+    return guard([&]() -> int { return ctx ? eng(ctx)->shard_end() : fail(PHX_E_INVALID, "null context"); });
+}
+
+PHX_API int phx_nccl_unique_id(uint8_t *out, uint32_t n) {
+    return guard([&]() -> int {
+        std::string why;
+        const NcclApi *api = nccl_api(&why);
+        if (!api)
+            return fail(PHX_E_UNSUPPORTED, why);
+        if (!out || n < sizeof(ncclUniqueId))
+            return fail(PHX_E_INVALID, "need 128 bytes for the NCCL unique id");
+        ncclUniqueId id;
+        ncclResult_t r = api->GetUniqueId(&id);
+        if (r != ncclSuccess)
+            return fail(PHX_E_CUDA, std::string("ncclGetUniqueId: ") + api->GetErrorString(r));
+        std::memcpy(out, &id, sizeof(id));
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_shard_nccl(void *ctx, const uint8_t *id) {
+    return guard([&]() -> int { return ctx ? eng(ctx)->shard_nccl_init(id) : fail(PHX_E_INVALID, "null context"); });
+}
+
+PHX_API int phx_shard_round(void *ctx) {
+    return guard([&]() -> int { return ctx ? eng(ctx)->shard_round() : fail(PHX_E_INVALID, "null context"); });
 }
 
 PHX_API int phx_scan_noalloc(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *total, uint64_t stream) {

@@ -46,6 +46,7 @@ void DevBuf::release() {
 Engine::~Engine() {
     if (st)
         cudaStreamSynchronize(st);
+    shard_release();
     invalidate_graph();
     for (auto &e : events)
         if (e)
@@ -404,6 +405,10 @@ LaunchCtx Engine::lc() const {
     l.nee_bases = d_nee_bases.as<u32>();
     l.total_nee = total_nee;
     l.nee_defer = tune.nee_wavefront ? 1u : 0u;
+    l.pix_lo = shard.world > 1 ? shard.pix_lo : 0u;
+    l.pix_hi = shard.world > 1 ? shard.pix_hi : total_pixels;
+    l.emit_lo = shard.world > 1 ? shard.emit_lo : 0u;
+    l.emit_hi = shard.world > 1 ? shard.emit_hi : total_emit;
     return l;
 }
 
@@ -617,6 +622,8 @@ int Engine::set_active(uint32_t scene, bool on) {
 }
 
 int Engine::plain_round() {
+    if (shard.world > 1)
+        return fail(PHX_E_STATE, "a sharded context renders with phx_shard_round or phx_shard_begin/_end");
     if (!any_active())
         return PHX_OK;
     enq_seeds();
@@ -687,6 +694,8 @@ void Engine::count_round(uint32_t rounds) {
 }
 
 int Engine::graph_rounds(uint32_t rounds) {
+    if (shard.world > 1)
+        return fail(PHX_E_STATE, "a sharded context renders with phx_shard_round or phx_shard_begin/_end");
     adjoint_invalidate();
     if (!any_active())
         return PHX_OK;
@@ -714,6 +723,8 @@ int Engine::graph_rounds(uint32_t rounds) {
 }
 
 int Engine::seeded_round(uint32_t seed) {
+    if (shard.world > 1)
+        return fail(PHX_E_STATE, "a sharded context renders with phx_shard_round or phx_shard_begin/_end");
     adjoint_invalidate();
     if (!any_active())
         return PHX_OK;
@@ -746,6 +757,8 @@ int Engine::upload_descs() {
 }
 
 int Engine::autotune(uint32_t rounds, phx_tuning *chosen) {
+    if (shard.world > 1)
+        return fail(PHX_E_STATE, "a sharded context renders with phx_shard_round or phx_shard_begin/_end");
     if (!any_active())
         return fail(PHX_E_STATE, "no active scene to tune on");
     if (rounds == 0 || rounds > 64)

@@ -58,6 +58,12 @@ enum Stage {
     ST__N
 };
 
+// One image over several GPUs: this rank's pixel and photon-path ranges (engine_shard.cu).
+struct ShardState {
+    uint32_t rank = 0, world = 1;
+    uint32_t pix_lo = 0, pix_hi = 0, emit_lo = 0, emit_hi = 0;
+};
+
 class Engine {
   public:
     ~Engine();
@@ -91,6 +97,16 @@ class Engine {
     // Picks the launch tuning that minimises the time of a graph-replayed round (coordinate descent
     // over the result-neutral knobs); the SPPM state is saved and restored around the trials.
     int autotune(uint32_t rounds_per_trial, phx_tuning *chosen);
+
+    // sharded rendering of one image (engine_shard.cu)
+    ShardState shard;
+    int set_shard(uint32_t rank, uint32_t world);
+    int shard_begin(uint32_t *n_local);
+    int shard_get_photons(float *pos4, uint32_t *pd2, uint32_t n);
+    int shard_put_photons(const float *pos4, const uint32_t *pd2, uint32_t n_all);
+    int shard_end();
+    int shard_nccl_init(const uint8_t *id);
+    int shard_round();
     bool any_active() const;
 
     // differentiation (single-scene engines; engine_adjoint.cu)
@@ -133,6 +149,12 @@ class Engine {
     void count_round(uint32_t rounds);
 
     int upload_descs();
+    int set_photon_total(uint32_t n);
+    void shard_release();
+    void *nccl_comm = nullptr; // ncclComm_t once attached
+    DevBuf sh_pos, sh_pd, sh_cnt;
+    uint32_t shard_n_local = 0, shard_n_all = 0;
+    int shard_phase = 0;
     // adjoint state: per round seeds, search radii² and SPPM ratios of the forward pass
     DevBuf adj_seeds, adj_r2, adj_ratio, adj_k, adj_img, adj_g, adj_gT, adj_gA, adj_gphi, adj_slot_pow, adj_ph_pow,
         adj_grad;

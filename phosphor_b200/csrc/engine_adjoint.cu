@@ -81,8 +81,8 @@ int Engine::set_lights(const phx_light *l, uint32_t n) {
 }
 
 int Engine::adjoint_forward(uint32_t rounds, float *image) {
-    if (sc.size() != 1)
-        return fail(PHX_E_UNSUPPORTED, "the adjoint is only available on single-scene contexts");
+    if (sc.size() != 1 || shard.world > 1)
+        return fail(PHX_E_UNSUPPORTED, "the adjoint is only available on single-scene, unsharded contexts");
     if (rounds == 0 || rounds > 4096)
         return fail(PHX_E_INVALID, "rounds must be 1..4096");
     SceneSlot &S = sc[0];

@@ -75,8 +75,8 @@ PHX_DI u32 emit_path(const SceneDesc &sc, u32 seed, u32 tid, const EmitOut &out,
 }
 
 __global__ void __launch_bounds__(128) k_emit(LaunchCtx lc, EmitOut out) {
-    u32 gid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= lc.total_emit)
+    u32 gid = lc.emit_lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= lc.emit_hi)
         return;
     u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.emit_bases, lc.n_scenes, gid);
     const SceneDesc &sc = lc.scenes[s];
@@ -171,8 +171,8 @@ __global__ void __launch_bounds__(128) k_emit_persistent(LaunchCtx lc, EmitOut o
                 base = atomicAdd(queue, (u32)__popc(need));
             base = __shfl_sync(0xffffffffu, base, leader);
             if (!active && !exhausted) {
-                const u32 gid = base + __popc(need & lt_mask);
-                if (gid < lc.total_emit) {
+                const u32 gid = lc.emit_lo + base + __popc(need & lt_mask);
+                if (gid < lc.emit_hi) {
                     const u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.emit_bases, lc.n_scenes, gid);
                     const SceneDesc *sc = lc.scenes + s;
                     pp_start(p, sc, __ldg(&lc.seeds[s]), gid - sc->emit_base, gid);
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(128) k_emit_persistent(LaunchCtx lc, EmitOut o
 
 void launch_emit(const LaunchCtx &lc, const EmitOut &out, int block, int persistent, int blocks_per_sm, u32 *queue,
                  cudaStream_t st) {
-    if (lc.total_emit == 0)
+    if (lc.emit_hi <= lc.emit_lo)
         return;
     if (persistent && queue && !out.slot_pow) {
         cudaMemsetAsync(queue, 0, sizeof(u32), st);
@@ -211,7 +211,7 @@ void launch_emit(const LaunchCtx &lc, const EmitOut &out, int block, int persist
         k_emit_persistent<<<grid, 128, 0, st>>>(lc, out, queue);
     } else {
         (void)block;
-        u32 grid = (lc.total_emit + 127) / 128;
+        u32 grid = (lc.emit_hi - lc.emit_lo + 127) / 128;
         k_emit<<<grid, 128, 0, st>>>(lc, out);
     }
 }

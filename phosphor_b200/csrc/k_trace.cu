@@ -146,8 +146,8 @@ PHX_DI void trace_pixel(const SceneDesc &sc, u32 seed, u32 tid, const TraceOut &
 }
 
 __global__ void __launch_bounds__(128) k_trace(LaunchCtx lc, TraceOut out) {
-    u32 gid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= lc.total_pixels)
+    u32 gid = lc.pix_lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= lc.pix_hi)
         return;
     u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gid);
     const SceneDesc &sc = lc.scenes[s];
@@ -420,8 +420,8 @@ __global__ void __launch_bounds__(128) k_trace_persistent(LaunchCtx lc, TraceOut
                 base = atomicAdd(queue, (u32)__popc(need));
             base = __shfl_sync(0xffffffffu, base, leader);
             if (!active && !exhausted) {
-                const u32 gid = base + __popc(need & lt_mask);
-                if (gid < lc.total_pixels) {
+                const u32 gid = lc.pix_lo + base + __popc(need & lt_mask);
+                if (gid < lc.pix_hi) {
                     const u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gid);
                     const SceneDesc *sc = lc.scenes + s;
                     if (sc->active) { // a retired scene's pixel is skipped; the lane refills next step
@@ -511,7 +511,7 @@ void launch_nee_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t s
 
 void launch_trace(const LaunchCtx &lc, const TraceOut &out, int block, int persistent, int blocks_per_sm, u32 *queue,
                   cudaStream_t st) {
-    if (lc.total_pixels == 0)
+    if (lc.pix_hi <= lc.pix_lo)
         return;
     if (persistent && queue) {
         cudaMemsetAsync(queue, 0, sizeof(u32), st);
@@ -519,7 +519,7 @@ void launch_trace(const LaunchCtx &lc, const TraceOut &out, int block, int persi
         k_trace_persistent<<<grid, 128, 0, st>>>(lc, out, queue);
     } else {
         (void)block;
-        u32 grid = (lc.total_pixels + 127) / 128;
+        u32 grid = (lc.pix_hi - lc.pix_lo + 127) / 128;
         k_trace<<<grid, 128, 0, st>>>(lc, out);
     }
 }

@@ -24,6 +24,8 @@ struct LaunchCtx {
     const u32 *nee_bases;    // device, n_scenes+1 prefix offsets of deferred-NEE sample slots
     u32 total_nee;           // sum over scenes of pixels * direct_samples
     u32 nee_defer;           // 1: diffuse-hit NEE shadow rays go to the shadow wavefront
+    u32 pix_lo, pix_hi;      // global pixels the camera pass traces (all, or one shard's range)
+    u32 emit_lo, emit_hi;    // global photon paths the photon pass emits
 };
 
 struct TraceOut {

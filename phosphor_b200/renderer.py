@@ -9,6 +9,7 @@ parity can be checked).  Every call goes through the C ABI; there is no Python o
 from __future__ import annotations
 
 import ctypes as C
+import os
 import dataclasses
 import struct
 import time
@@ -115,6 +116,28 @@ class SceneData:
         sc = A.Scene.from_buffer_copy(self.scene)
         sc.camera = camera
         return SceneData(sc, owner=None, keep=(self,))
+
+
+def _prefer_bundled_nccl() -> None:
+    """Points PHX_NCCL_LIB at the NCCL that this Python environment bundles (the one torch links),
+    so that the library and a framework in the same process share one NCCL."""
+    if os.environ.get("PHX_NCCL_LIB"):
+        return
+    import importlib.util
+    spec = importlib.util.find_spec("nvidia.nccl")
+    for loc in (spec.submodule_search_locations or []) if spec else []:
+        cand = Path(loc) / "lib" / "libnccl.so.2"
+        if cand.exists():
+            os.environ["PHX_NCCL_LIB"] = str(cand)
+            return
+
+
+def nccl_unique_id() -> bytes:
+    """A fresh NCCL unique id (128 bytes) for phx_shard_nccl, made on one rank and sent to all."""
+    _prefer_bundled_nccl()
+    buf = (C.c_uint8 * 128)()
+    A.check(A.load().phx_nccl_unique_id(buf, 128))
+    return bytes(buf)
 
 
 def bvh_build(scene: SceneData) -> tuple[np.ndarray, int]:
@@ -304,6 +327,38 @@ class Renderer:
 
     def stream(self) -> int:
         return int(self._lib.phx_get_stream(self._need()))
+
+    # one image over several GPUs (no reference counterpart; see include/phx.h)
+    def shard(self, rank: int, world: int) -> None:
+        A.check(self._lib.phx_shard(self._need(), rank, world))
+
+    def shard_begin(self) -> int:
+        """Seed, camera pass over this rank's pixels, photon pass over its paths; photons stored."""
+        n = C.c_uint32()
+        A.check(self._lib.phx_shard_begin(self._need(), C.byref(n)))
+        return n.value
+
+    def shard_get_photons(self, n: int) -> tuple[np.ndarray, np.ndarray]:
+        pos = np.empty((n, 4), np.float32)
+        pd = np.empty((n, 2), np.uint32)
+        A.check(self._lib.phx_shard_get_photons(self._need(), pos.ctypes.data, pd.ctypes.data, n))
+        return pos, pd
+
+    def shard_put_photons(self, pos: np.ndarray, pd: np.ndarray) -> None:
+        pos = np.ascontiguousarray(pos, np.float32)
+        pd = np.ascontiguousarray(pd, np.uint32)
+        A.check(self._lib.phx_shard_put_photons(self._need(), pos.ctypes.data, pd.ctypes.data, len(pos)))
+
+    def shard_end(self) -> None:
+        A.check(self._lib.phx_shard_end(self._need()))
+
+    def shard_nccl(self, unique_id: bytes) -> None:
+        _prefer_bundled_nccl()
+        buf = (C.c_uint8 * 128).from_buffer_copy(unique_id)
+        A.check(self._lib.phx_shard_nccl(self._need(), buf))
+
+    def shard_round(self) -> None:
+        A.check(self._lib.phx_shard_round(self._need()))
 
     # differentiation (no reference counterpart; see include/phx.h)
     def n_params(self) -> int:
