@@ -423,6 +423,14 @@ class Batch:
     def iterate(self, rounds: int, graph: bool = True) -> None:
         A.check(self._lib.phx_batch_iterate(self.h, rounds, 1 if graph else 0))
 
+    def tuning(self) -> A.Tuning:
+        t = A.Tuning()
+        A.check(self._lib.phx_get_tuning(self.h, C.byref(t)))
+        return t
+
+    def set_tuning(self, t: A.Tuning) -> None:
+        A.check(self._lib.phx_set_tuning(self.h, C.byref(t)))
+
     def set_active(self, s: int, active: bool) -> None:
         """Retire (False) or resume a scene: retired scenes cost no work in later rounds."""
         A.check(self._lib.phx_batch_set_active(self.h, s, int(active)))
