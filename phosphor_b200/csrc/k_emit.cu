@@ -17,6 +17,12 @@
 #include "dev_shading.cuh"
 #include "kernels.hpp"
 
+// Minimum resident blocks per SM asked of the compiler (caps registers per thread at 64): 8 blocks
+// per SM measured fastest for the photon kernel (6.3 -> 5.4 ms; 10 or 12 spill too much).
+#ifndef PHX_EMIT_MINB
+#define PHX_EMIT_MINB 8
+#endif
+
 namespace phx {
 
 PHX_DI u32 emit_path(const SceneDesc &sc, u32 seed, u32 tid, const EmitOut &out, u32 *overflow) {
@@ -156,7 +162,7 @@ PHX_DI bool pp_advance(PhotonPath &p, bool hit, const Hit &h, const EmitOut &out
     return p.depth < sc.max_bounces;
 }
 
-__global__ void __launch_bounds__(128) k_emit_persistent(LaunchCtx lc, EmitOut out, u32 *queue) {
+__global__ void __launch_bounds__(128, PHX_EMIT_MINB) k_emit_persistent(LaunchCtx lc, EmitOut out, u32 *queue) {
     const u32 lane = threadIdx.x & 31u;
     const u32 lt_mask = (1u << lane) - 1u;
     u32 ovf = 0;

@@ -110,7 +110,12 @@ PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
     }
 }
 
-__global__ void __launch_bounds__(128) k_gather(LaunchCtx lc, GatherBufs g) {
+// 12 resident blocks per SM (42 registers, ~100 bytes of spills): the photon loop is latency-bound
+// and more warps hide it better (7.3 -> 6.4 ms; 16 blocks spill more and measured slower).
+#ifndef PHX_GATHER_MINB
+#define PHX_GATHER_MINB 12
+#endif
+__global__ void __launch_bounds__(128, PHX_GATHER_MINB) k_gather(LaunchCtx lc, GatherBufs g) {
     u32 gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= lc.total_pixels)
         return;

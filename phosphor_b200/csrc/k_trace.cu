@@ -26,6 +26,17 @@
 #include "dev_shading.cuh"
 #include "kernels.hpp"
 
+// Minimum resident blocks per SM asked of the compiler, which caps registers per thread (64 at 8
+// blocks of 128 threads).  Both traversal kernels are latency-bound: 8 blocks per SM (with a few
+// hundred bytes of spills to L1) measured faster than 4-7 register-limited blocks, and faster than
+// 10-12 blocks with heavier spills (camera kernel 8.5 -> 7.7 ms, shadow 8.8 -> 7.8 ms).
+#ifndef PHX_TRACE_MINB
+#define PHX_TRACE_MINB 8
+#endif
+#ifndef PHX_SHADOW_MINB
+#define PHX_SHADOW_MINB 8
+#endif
+
 namespace phx {
 
 struct TraceResult {
@@ -404,7 +415,7 @@ PHX_DI bool cp_advance(CameraPath &p, bool hit, const Hit &h, const TraceOut &ou
     return cp_after_nee(p, out);
 }
 
-__global__ void __launch_bounds__(128) k_trace_persistent(LaunchCtx lc, TraceOut out, u32 *queue) {
+__global__ void __launch_bounds__(128, PHX_TRACE_MINB) k_trace_persistent(LaunchCtx lc, TraceOut out, u32 *queue) {
     const u32 lane = threadIdx.x & 31u;
     const u32 lt_mask = (1u << lane) - 1u;
     u32 ovf = 0;
@@ -449,7 +460,7 @@ __global__ void __launch_bounds__(128) k_trace_persistent(LaunchCtx lc, TraceOut
 // ---- shadow wavefront ---------------------------------------------------------------------------
 // One thread per recorded NEE sample; the ds samples of a pixel are consecutive threads, so a warp
 // traces shadow rays from one or two hit points toward the same light: coherent traversal.
-__global__ void __launch_bounds__(128) k_shadow(LaunchCtx lc, TraceOut out) {
+__global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow(LaunchCtx lc, TraceOut out) {
     const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= lc.total_nee)
         return;
