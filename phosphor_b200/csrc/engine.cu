@@ -1117,7 +1117,7 @@ int Engine::info(uint32_t s, phx_info *o) {
     o->trav_inner_nodes = S.trav_inner;
     // seeds, trace, [shadow, resolve], emit, count scan, compaction, hash, cell scan, 3 per sort
     // pass, records, gather
-    o->kernels_per_round = 9 + 3 * o->sort_passes + (tune.nee_wavefront ? 2 : 0);
+    o->kernels_per_round = 9 + 3 * o->sort_passes + (tune.nee_wavefront ? 3 : 0);
     CK(cudaStreamSynchronize(st));
     uint32_t v[2] = {0, 0};
     CK(cudaMemcpy(&v[0], d_ovf.p, 4, cudaMemcpyDeviceToHost));

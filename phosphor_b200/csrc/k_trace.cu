@@ -54,9 +54,17 @@ PHX_DI void write_result(const TraceOut &out, u32 gpix, const TraceResult &r) {
 
 // Deferred diffuse-hit NEE (trace_rays.cl:103-118).  The reference's path ends after this loop
 // and its RNG draws (light choice, light point) never depend on the shadow rays' outcome, so the
-// loop is split: here the samples are drawn in order and each shadow ray is recorded; the shadow
-// wavefront traces them; the resolve kernel sums the contributions in sample order.
-PHX_SHADE_NEE void record_nee(const SceneDesc &sc, Rng *rng, float4 pos, float4 sn, float4 base, const TraceOut &out,
+// loop is split in three kernels: k_nee_sample draws the samples in order and records each shadow
+// ray; the shadow wavefront traces them; the resolve kernel sums the contributions in sample order.
+// The camera kernels only leave the pixel's RNG state and shading normal in its first sample slot
+// (stash_nee): drawing the samples there would run the light-sampling code for one lane of a warp
+// at a time, while k_nee_sample runs it for 32 diffuse hit points together.
+PHX_DI void stash_nee(const TraceOut &out, u32 slot, Rng rng, float4 sn) {
+    out.nee_ray[slot] = sn;
+    out.nee_val[slot] = f4(__uint_as_float(rng.state), 0.0f, 0.0f, 0.0f);
+}
+
+PHX_DI void record_nee(const SceneDesc &sc, Rng *rng, float4 pos, float4 sn, float4 base, const TraceOut &out,
                        u32 slot) {
     for (u32 d = 0; d < sc.direct_samples; d++, slot++) {
         LightFragment f;
@@ -107,8 +115,7 @@ PHX_DI void trace_pixel(const SceneDesc &sc, u32 seed, u32 tid, const TraceOut &
         BsdfSample bs = sample_bsdf(&rng, ctx, ctx.shading_normal, sh.normal, view, &ior, sh.front_face);
         if (bs.event == BSDF_DIFFUSE) {
             if (defer) {
-                record_nee(sc, &rng, sh.position, ctx.shading_normal, ctx.base_color, out,
-                           sc.nee_base + tid * sc.direct_samples);
+                stash_nee(out, sc.nee_base + tid * sc.direct_samples, rng, ctx.shading_normal);
                 direct = f4(ctx.occlusion, 0.0f, 0.0f, 0.0f); // the resolve kernel completes it
             } else {
                 float4 sum = zero4();
@@ -394,7 +401,7 @@ PHX_DI bool cp_advance(CameraPath &p, bool hit, const Hit &h, const TraceOut &ou
     if (bs.event == BSDF_DIFFUSE) {
         p.nee_kind = NEE_DIFFUSE;
         if (defer) {
-            record_nee(sc, &p.rng, p.pos, p.sn, p.base, out, sc.nee_base + p.tid * sc.direct_samples);
+            stash_nee(out, sc.nee_base + p.tid * sc.direct_samples, p.rng, p.sn);
             cp_finish(p, out, true, true);
             return false;
         }
@@ -507,10 +514,31 @@ __global__ void __launch_bounds__(256) k_nee_resolve(LaunchCtx lc, TraceOut out)
     out.direct[gpix] = out.throughput[gpix] * occl * (sum / (float)ds);
 }
 
+// Draws the diffuse-NEE samples of every pixel with a diffuse hit point (one thread per pixel),
+// from the RNG state and shading normal the camera pass left in the pixel's first sample slot.
+__global__ void __launch_bounds__(128) k_nee_sample(LaunchCtx lc, TraceOut out) {
+    const u32 gpix = lc.pix_lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (gpix >= lc.pix_hi)
+        return;
+    if (out.emission[gpix].w != 1.0f)
+        return; // no diffuse hit point
+    const u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gpix);
+    const SceneDesc &sc = lc.scenes[s];
+    if (!sc.active)
+        return;
+    const u32 slot = sc.nee_base + (gpix - sc.pixel_base) * sc.direct_samples;
+    const float4 sn = out.nee_ray[slot];
+    Rng rng;
+    rng.state = __float_as_uint(out.nee_val[slot].x);
+    record_nee(sc, &rng, out.pos[gpix], sn, out.base_color[gpix], out, slot);
+}
+
 void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int block, cudaStream_t st) {
     (void)block;
     if (!lc.nee_defer || lc.total_nee == 0)
         return;
+    if (lc.pix_hi > lc.pix_lo)
+        k_nee_sample<<<(lc.pix_hi - lc.pix_lo + 127) / 128, 128, 0, st>>>(lc, out);
     k_shadow<<<(lc.total_nee + 127) / 128, 128, 0, st>>>(lc, out);
 }
 
