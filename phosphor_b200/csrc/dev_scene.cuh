@@ -162,14 +162,14 @@ PHX_DI void box2(const float4 &a, const float4 &b, const float4 &c, float ix, fl
     *hr = rnear <= rfar;
 }
 
-// Slab test of one child of a 4-wide node; returns its entry distance, or +inf on a miss.
-PHX_DI float box1(float mnx, float mxx, float mny, float mxy, float mnz, float mxz, float ix, float iy, float iz,
+// Slab test of one child of a 4-wide node, given per axis the plane the ray enters first (nx, ny,
+// nz) and the one it leaves by (fx, fy, fz), picked once per ray from the sign of its direction;
+// returns the entry distance, or +inf on a miss.  A slab whose distances are NaN (a zero direction
+// component with the origin's inf products) is ignored by fmaxf / fminf: never pruned wrongly.
+PHX_DI float box1(float nx, float fx, float ny, float fy, float nz, float fz, float ix, float iy, float iz,
                   float oix, float oiy, float oiz, float t_min, float t_max) {
-    float x0 = __fmaf_rn(mnx, ix, -oix), x1 = __fmaf_rn(mxx, ix, -oix);
-    float y0 = __fmaf_rn(mny, iy, -oiy), y1 = __fmaf_rn(mxy, iy, -oiy);
-    float z0 = __fmaf_rn(mnz, iz, -oiz), z1 = __fmaf_rn(mxz, iz, -oiz);
-    float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), t_min));
-    float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), t_max));
+    float tn = fmaxf(fmaxf(__fmaf_rn(nx, ix, -oix), __fmaf_rn(ny, iy, -oiy)), fmaxf(__fmaf_rn(nz, iz, -oiz), t_min));
+    float tf = fminf(fminf(__fmaf_rn(fx, ix, -oix), __fmaf_rn(fy, iy, -oiy)), fminf(__fmaf_rn(fz, iz, -oiz), t_max));
     return tn <= tf ? tn : __int_as_float(0x7f800000);
 }
 
@@ -196,6 +196,8 @@ PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, floa
     constexpr i32 POP = 0x7fffffff;
     const float ix = 1.0f / d.x, iy = 1.0f / d.y, iz = 1.0f / d.z;
     const float oix = o.x * ix, oiy = o.y * iy, oiz = o.z * iz;
+    // 4-wide nodes: offsets of the entry-plane rows {minx, maxx, miny, maxy, minz, maxz}
+    const int px = ix >= 0.0f ? 0 : 1, py = iy >= 0.0f ? 2 : 3, pz = iz >= 0.0f ? 4 : 5;
     float closest = t_max;
     i32 best = -1, best_rank = -1;
     float bu = 0.0f, bv = 0.0f;
@@ -210,11 +212,11 @@ PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, floa
             continue;
         if (node >= 0 && sc.wide) { // 4-wide node: descend into the nearest hit child, stack the rest
             const float4 *wn = sc.cnodes + 7 * (size_t)node;
-            const float4 mnx = __ldg(wn + 0), mxx = __ldg(wn + 1), mny = __ldg(wn + 2), mxy = __ldg(wn + 3);
-            const float4 mnz = __ldg(wn + 4), mxz = __ldg(wn + 5);
+            const float4 mnx = __ldg(wn + px), mxx = __ldg(wn + (1 - px)), mny = __ldg(wn + py);
+            const float4 mxy = __ldg(wn + (5 - py)), mnz = __ldg(wn + pz), mxz = __ldg(wn + (9 - pz));
             const int4 ch = __ldg(reinterpret_cast<const int4 *>(wn + 6));
-            // An empty slot (reference POP) never counts as hit: its box cannot be relied on to miss,
-            // since the slab test orders each pair of plane distances itself.
+            // (mnx.. now hold the entry planes, mxx.. the exit planes.)  An empty slot (reference POP)
+            // never counts as hit, whatever its box.
             const float NOHIT = __int_as_float(0x7f800000);
             float t0 = ch.x == POP ? NOHIT
                                    : box1(mnx.x, mxx.x, mny.x, mxy.x, mnz.x, mxz.x, ix, iy, iz, oix, oiy, oiz, t_min,
