@@ -318,7 +318,8 @@ typedef struct phx_tuning {
     uint32_t nee_wavefront;     /* 1 = diffuse-hit NEE shadow rays traced by a separate wavefront */
     uint32_t concurrent_passes; /* 1 = in the captured graph the camera pass and the photon pass of a
                                    round run on two branches (they only share the round seed) */
-    uint32_t reserved[4];
+    uint32_t gather_sorted;     /* 1 = the gather visits pixels grouped by photon-grid cell */
+    uint32_t reserved[3];
 } phx_tuning;
 PHX_API int phx_get_tuning(void *ctx, phx_tuning *out);
 PHX_API int phx_set_tuning(void *ctx, const phx_tuning *in);

@@ -63,7 +63,7 @@ Engine::~Engine() {
                      &d_err, &d_ovf, &d_queue, &d_ntotal,
                      &flux, &weight, &radiance, &slot_pos, &slot_pd, &counts, &offsets, &ph_pos, &ph_pd, &keys,
                      &cell_count, &cell_start, &sk0, &sk1, &sv0, &sv1, &s_posdir, &s_power, &scan_scr, &radix_scr,
-                     &img_rgb, &img_ldr, &adj_seeds, &adj_r2, &adj_ratio, &adj_k, &adj_img, &adj_g, &adj_gT,
+                     &img_rgb, &img_ldr, &pk_keys, &pk_t0, &pk_t1, &pk_v0, &pk_v1, &pk_scr, &d_npix, &adj_seeds, &adj_r2, &adj_ratio, &adj_k, &adj_img, &adj_g, &adj_gT,
                      &adj_gA, &adj_gphi, &adj_slot_pow, &adj_ph_pow, &adj_grad};
     for (auto *b : all)
         b->release();
@@ -375,6 +375,16 @@ int Engine::create(const phx_scene *scenes, const phx_params *params, uint32_t n
         (r = radix_scr.alloc(radix_scratch_bytes(N, key_bits))))
         return r;
     perm = sv0.as<u32>();
+    // gather order: sort the pixels by (cell, octant) key; needs the composite key to fit 32 bits
+    pix_key_bits = key_bits + 3 <= 32 ? key_bits + 3 : 0;
+    if (pix_key_bits) {
+        const uint32_t Pn = total_pixels;
+        if ((r = pk_keys.alloc(4 * (size_t)Pn)) || (r = pk_t0.alloc(4 * (size_t)Pn)) ||
+            (r = pk_t1.alloc(4 * (size_t)Pn)) || (r = pk_v0.alloc(4 * (size_t)Pn)) ||
+            (r = pk_v1.alloc(4 * (size_t)Pn)) || (r = pk_scr.alloc(radix_scratch_bytes(Pn, pix_key_bits))) ||
+            (r = upload(d_npix, &Pn, 4)))
+            return r;
+    }
     CK(cudaMallocHost((void **)&h_pinned, 4096));
     tune.trace_block = 128;
     tune.emit_block = 128;
@@ -384,6 +394,7 @@ int Engine::create(const phx_scene *scenes, const phx_params *params, uint32_t n
     tune.persistent = 1;
     tune.nee_wavefront = 1;
     tune.concurrent_passes = 0;
+    tune.gather_sorted = 1;
     for (uint32_t i = 0; i < n; i++)
         if (params[i].flags & PHX_F_SIMPLE_TRAVERSAL)
             tune.persistent = 0;
@@ -497,10 +508,17 @@ void Engine::enq_hash_sort() {
 void Engine::enq_gather() {
     adjoint_invalidate();
     ev(ST_GATHER, false);
+    const u32 *order = nullptr;
+    if (tune.gather_sorted && pix_key_bits) {
+        launch_pixel_keys(lc(), hp[0].as<float4>(), hp[5].as<float4>(), pk_keys.as<u32>(), st);
+        launch_radix_sort(pk_keys.as<u32>(), pk_t0.as<u32>(), pk_t1.as<u32>(), pk_v0.as<u32>(), pk_v1.as<u32>(),
+                          &pix_order, d_npix.as<u32>(), total_pixels, pix_key_bits, pk_scr.p, d_err.as<u32>(), st);
+        order = pix_order;
+    }
     GatherBufs g{hp[0].as<float4>(), hp[1].as<float4>(), hp[2].as<float4>(), hp[3].as<float4>(),
                  hp[4].as<float4>(), hp[5].as<float4>(), s_posdir.as<float4>(), s_power.as<u32>(),
                  cell_start.as<u32>(), (u32)max_photons, flux.as<float4>(), weight.as<float>(),
-                 radiance.as<float4>(), rec_r2, rec_ratio};
+                 radiance.as<float4>(), rec_r2, rec_ratio, order};
     launch_gather(lc(), g, (int)tune.gather_block, st);
     ev(ST_GATHER, true);
 }
@@ -829,6 +847,7 @@ int Engine::autotune(uint32_t rounds, phx_tuning *chosen) {
         knob(&phx_tuning::emit_blocks_per_sm, {2u, 4u, 6u, 8u, 12u, 16u});
     }
     knob(&phx_tuning::concurrent_passes, {0u, 1u});
+    knob(&phx_tuning::gather_sorted, {1u, 0u});
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     tune = best;
@@ -1117,7 +1136,8 @@ int Engine::info(uint32_t s, phx_info *o) {
     o->trav_inner_nodes = S.trav_inner;
     // seeds, trace, [shadow, resolve], emit, count scan, compaction, hash, cell scan, 3 per sort
     // pass, records, gather
-    o->kernels_per_round = 9 + 3 * o->sort_passes + (tune.nee_wavefront ? 3 : 0);
+    o->kernels_per_round = 9 + 3 * o->sort_passes + (tune.nee_wavefront ? 3 : 0) +
+                           (tune.gather_sorted && pix_key_bits ? 1 + 3 * radix_passes(pix_key_bits) : 0);
     CK(cudaStreamSynchronize(st));
     uint32_t v[2] = {0, 0};
     CK(cudaMemcpy(&v[0], d_ovf.p, 4, cudaMemcpyDeviceToHost));

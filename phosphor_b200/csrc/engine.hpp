@@ -162,6 +162,11 @@ class Engine {
     bool adj_ready = false, adj_k_ready = false, in_adjoint = false;
     float *rec_r2 = nullptr, *rec_ratio = nullptr; // recording targets of the gather (forward pass)
 
+    // pixel order of the gather (pixels grouped by photon-grid cell)
+    DevBuf pk_keys, pk_t0, pk_t1, pk_v0, pk_v1, pk_scr, d_npix;
+    uint32_t pix_key_bits = 0; // 0: the gather runs in pixel order
+    u32 *pix_order = nullptr;
+
     u32 *perm = nullptr;
     u32 *h_pinned = nullptr;
     cudaGraph_t graph = nullptr, graph_host = nullptr;

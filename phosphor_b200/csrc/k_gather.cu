@@ -119,9 +119,42 @@ __global__ void __launch_bounds__(128, PHX_GATHER_MINB) k_gather(LaunchCtx lc, G
     u32 gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= lc.total_pixels)
         return;
+    if (g.order)
+        gid = __ldg(&g.order[gid]);
     u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gid);
     if (lc.scenes[s].active)
         gather_pixel(lc.scenes[s], gid, g);
+}
+
+// Pixels whose hit points share a photon-grid cell (and an octant of it) visit the same cells and
+// skip the same ones, so gathering them in one warp keeps its lanes in step and lets them share
+// every photon record load.  Each pixel's own computation does not change.
+__global__ void __launch_bounds__(256) k_pixel_keys(LaunchCtx lc, const float4 *hp_pos, const float4 *hp_emission,
+                                                    u32 *keys) {
+    const u32 gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= lc.total_pixels)
+        return;
+    u32 key = 0;
+    if (hp_emission[gid].w == 1.0f) {
+        const u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gid);
+        const SceneDesc &sc = lc.scenes[s];
+        const float4 p = hp_pos[gid];
+        const u32 h = get_hash(p.x, p.y, p.z, sc.grid);
+        if (h) {
+            const GridDev &gd = sc.grid;
+            const float fx = (p.x - gd.ox) / gd.cx, fy = (p.y - gd.oy) / gd.cy, fz = (p.z - gd.oz) / gd.cz;
+            const u32 oct = (fx - floorf(fx) >= 0.5f ? 1u : 0u) | (fy - floorf(fy) >= 0.5f ? 2u : 0u) |
+                            (fz - floorf(fz) >= 0.5f ? 4u : 0u);
+            key = ((sc.cell_base + h) << 3) | oct;
+        }
+    }
+    keys[gid] = key;
+}
+
+void launch_pixel_keys(const LaunchCtx &lc, const float4 *hp_pos, const float4 *hp_emission, u32 *keys,
+                       cudaStream_t st) {
+    if (lc.total_pixels)
+        k_pixel_keys<<<(lc.total_pixels + 255) / 256, 256, 0, st>>>(lc, hp_pos, hp_emission, keys);
 }
 
 void launch_gather(const LaunchCtx &lc, const GatherBufs &g, int block, cudaStream_t st) {
