@@ -50,7 +50,9 @@ CONFIGS = {
 METRIC = "Mphotons/s"
 # dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu capture of the full-size
 # workload (profiles/dram_traffic_caustic_1024.md)
-NCU_TRAFFIC = {"caustic": {"trace": 853_658_368, "shadow": 750_293_504, "emit": 163_459_584, "gather": 204_436_992}}
+# (the shadow stage: k_nee_sample + k_shadow; k_nee_resolve, under 5 % of the stage, not captured)
+NCU_TRAFFIC = {"caustic": {"trace": 1_329_052_672, "shadow": 1_608_642_560, "emit": 506_128_640,
+                           "gather": 225_226_240}}
 ALGO_STAGES = ["trace", "shadow", "emit", "emit_scan", "hash", "cell_scan", "sort", "records", "gather"]
 
 
@@ -188,8 +190,10 @@ def algorithmic_bytes(stage: str, P: int, Ne: int, Ns: int, C: int, scene_bytes:
     """Compulsory bytes per round of each stage: the hit-point, photon, cell and image records each
     stage must read or write once, plus the scene geometry for the traversal stages."""
     return {
-        "trace": 96 * P + 32 * P * ds + scene_bytes,
-        "shadow": 48 * P * ds + 48 * P + scene_bytes,
+        # camera pass: the hit point (96 B) and the NEE stash (32 B) per pixel
+        "trace": 96 * P + 32 * P + scene_bytes,
+        # NEE samples written (32 B), read and replaced by the shadow pass (32 + 16 B), summed (16 B)
+        "shadow": 96 * P * ds + 48 * P + scene_bytes,
         "emit": 24 * Ns + scene_bytes,
         "emit_scan": 8 * Ne + 48 * Ns,
         "hash": 16 * Ns + 4 * Ns + 4 * C + 8 * Ns,
