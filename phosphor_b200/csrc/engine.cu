@@ -62,7 +62,7 @@ Engine::~Engine() {
     DevBuf *all[] = {&d_desc, &d_pix_bases, &d_emit_bases, &d_nee_bases, &nee_ray, &nee_val, &d_seeds, &d_rng,
                      &d_err, &d_ovf, &d_queue, &d_ntotal,
                      &flux, &weight, &radiance, &slot_pos, &slot_pd, &counts, &offsets, &ph_pos, &ph_pd, &keys,
-                     &cell_count, &cell_start, &sk0, &sk1, &sv0, &sv1, &s_posdir, &s_power, &scan_scr, &radix_scr,
+                     &cell_count, &cell_start, &sk0, &sk1, &sv0, &sv1, &s_posdir, &s_power, &s_dir, &s_pow, &scan_scr, &radix_scr,
                      &img_rgb, &img_ldr, &pk_keys, &pk_t0, &pk_t1, &pk_v0, &pk_v1, &pk_scr, &d_npix, &adj_seeds, &adj_r2, &adj_ratio, &adj_k, &adj_img, &adj_g, &adj_gT,
                      &adj_gA, &adj_gphi, &adj_slot_pow, &adj_ph_pow, &adj_grad};
     for (auto *b : all)
@@ -370,7 +370,8 @@ int Engine::create(const phx_scene *scenes, const phx_params *params, uint32_t n
         (r = upload(cell_count, nullptr, 4 * C)) || (r = upload(cell_start, nullptr, 4 * C)) ||
         (r = sk0.alloc(4 * N)) || (r = sk1.alloc(4 * N)) || (r = upload(sv0, nullptr, 4 * N)) ||
         (r = upload(sv1, nullptr, 4 * N)) || (r = upload(s_posdir, nullptr, 16 * N)) ||
-        (r = upload(s_power, nullptr, 4 * N)) ||
+        (r = upload(s_power, nullptr, 4 * N)) || (r = upload(s_dir, nullptr, 16 * N)) ||
+        (r = upload(s_pow, nullptr, 16 * N)) ||
         (r = scan_scr.alloc(std::max(scan_scratch_bytes(E + 1), scan_scratch_bytes(C)))) ||
         (r = radix_scr.alloc(radix_scratch_bytes(N, key_bits))))
         return r;
@@ -500,7 +501,8 @@ void Engine::enq_hash_sort() {
     ev(ST_SORT, true);
     ev(ST_RECORDS, false);
     launch_sorted_records(perm, ph_pos.as<float4>(), ph_pd.as<uint2>(), d_ntotal.as<u32>(), max_photons,
-                          s_posdir.as<float4>(), s_power.as<u32>(), d_err.as<u32>(), st);
+                          s_posdir.as<float4>(), s_power.as<u32>(), s_dir.as<float4>(), s_pow.as<float4>(),
+                          d_err.as<u32>(), st);
     ev(ST_RECORDS, true);
     stage_state |= 4;
 }
@@ -517,8 +519,8 @@ void Engine::enq_gather() {
     }
     GatherBufs g{hp[0].as<float4>(), hp[1].as<float4>(), hp[2].as<float4>(), hp[3].as<float4>(),
                  hp[4].as<float4>(), hp[5].as<float4>(), s_posdir.as<float4>(), s_power.as<u32>(),
-                 cell_start.as<u32>(), (u32)max_photons, flux.as<float4>(), weight.as<float>(),
-                 radiance.as<float4>(), rec_r2, rec_ratio, order};
+                 s_dir.as<float4>(), s_pow.as<float4>(), cell_start.as<u32>(), (u32)max_photons,
+                 flux.as<float4>(), weight.as<float>(), radiance.as<float4>(), rec_r2, rec_ratio, order};
     launch_gather(lc(), g, (int)tune.gather_block, st);
     ev(ST_GATHER, true);
 }
@@ -1052,6 +1054,14 @@ int Engine::write_buffer(uint32_t s, int which, const void *src, uint64_t off, u
         CK(cudaMemcpy((char *)base + off, src, bytes, cudaMemcpyHostToDevice));
         return PHX_OK;
     };
+    // the gather reads each record's decoded direction and power: refresh them after host writes
+    auto decode_records = [&]() -> int {
+        launch_decode_records(s_posdir.as<float4>(), s_power.as<u32>(), max_photons, s_dir.as<float4>(),
+                              s_pow.as<float4>(), st);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+        return PHX_OK;
+    };
     const size_t P = d.n_pixels, N = max_photons;
     switch (which) {
     case PHX_BUF_HP_POS: case PHX_BUF_HP_NORMAL: case PHX_BUF_HP_THROUGHPUT: case PHX_BUF_HP_BASE_COLOR:
@@ -1066,9 +1076,11 @@ int Engine::write_buffer(uint32_t s, int which, const void *src, uint64_t off, u
         return put(weight.p, 4 * P);
     case PHX_BUF_PHOTON_POS:
         return put(ph_pos.p, 16 * N);
-    case PHX_BUF_SORTED_POWER:
+    case PHX_BUF_SORTED_POWER: {
         stage_state |= 4;
-        return put(s_power.p, 4 * N);
+        const int r = put(s_power.p, 4 * N);
+        return r ? r : decode_records();
+    }
     case PHX_BUF_CELL_START:
         stage_state |= 4;
         return put(cell_start.p, 4 * (size_t)d.n_cells);
@@ -1095,6 +1107,8 @@ int Engine::write_buffer(uint32_t s, int which, const void *src, uint64_t off, u
             }
             CK(cudaMemcpy(s_posdir.as<float4>() + e0, v.data(), 16 * ne, cudaMemcpyHostToDevice));
             stage_state |= 4;
+            if (int r = decode_records())
+                return r;
         } else {
             std::vector<uint2> v(ne);
             CK(cudaMemcpy(v.data(), ph_pd.as<uint2>() + e0, 8 * ne, cudaMemcpyDeviceToHost));

@@ -144,7 +144,7 @@ class Engine {
     DevBuf nee_ray, nee_val;
     DevBuf hp[6], flux, weight, radiance;
     DevBuf slot_pos, slot_pd, counts, offsets, ph_pos, ph_pd, keys, cell_count, cell_start;
-    DevBuf sk0, sk1, sv0, sv1, s_posdir, s_power, scan_scr, radix_scr, img_rgb, img_ldr;
+    DevBuf sk0, sk1, sv0, sv1, s_posdir, s_power, s_dir, s_pow, scan_scr, radix_scr, img_rgb, img_ldr;
     int capture(bool with_seeds, cudaGraph_t *g, cudaGraphExec_t *ge);
     void count_round(uint32_t rounds);
 

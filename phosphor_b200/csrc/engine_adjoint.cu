@@ -192,8 +192,8 @@ int Engine::adjoint_backward(const float *dl_dimage, float *grad, uint32_t n_gra
         ab.perm = perm;
         GatherBufs gbuf{hp[0].as<float4>(), hp[1].as<float4>(), hp[2].as<float4>(), hp[3].as<float4>(),
                         hp[4].as<float4>(), hp[5].as<float4>(), s_posdir.as<float4>(), s_power.as<u32>(),
-                        cell_start.as<u32>(), (u32)max_photons, flux.as<float4>(), weight.as<float>(),
-                        radiance.as<float4>(), nullptr, nullptr};
+                        s_dir.as<float4>(), s_pow.as<float4>(), cell_start.as<u32>(), (u32)max_photons,
+                        flux.as<float4>(), weight.as<float>(), radiance.as<float4>(), nullptr, nullptr};
         launch_gather_adj(lc(), gbuf, ab, st);
         launch_trace_adj(lc(), ab, st);
         launch_emit_adj(lc(), ab, st);

@@ -2,9 +2,9 @@
 // (kernels/gather_flux.cl:5-78, gather_photon_flux in include/common/photon_hash.h:56-103), and
 // the image formation of src/renderer/output.cpp:40-83.
 //
-// Photons are read in cell order from the sorted records {x, y, z, octahedral dir bits} (16 B,
-// one load answers the radius test and the orientation test) plus the RGBE power word, which is
-// only loaded for photons inside the radius.  Each pixel accumulates its 27 cells in the
+// Photons are read in cell order from the sorted records {x, y, z, octahedral dir bits} (16 B, one
+// load answers the radius test); the direction and power, decoded once per round when the records
+// are written, are only loaded for photons inside the radius.  Each pixel accumulates its 27 cells in the
 // reference's cell order and each cell in sorted (= canonical) order, in one thread with no float
 // atomics, so the sum is deterministic and equal to the reference's sequential sum.  cell_end is
 // not materialised: the cells are contiguous, so end(h) = start(h+1).
@@ -51,10 +51,10 @@ PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
         const float dx = pos.x - p.x, dy = pos.y - p.y, dz = pos.z - p.z, dw = pos.w - 0.0f;
         const float dsq = ((dx * dx + dy * dy) + dz * dz) + dw * dw;
         if (dsq < r_sq) {
-            const float4 pd = decode_oct(__float_as_uint(p.w));
+            const float4 pd = __ldg(&g.s_dir[k]); // decode_oct(p.w), decoded once per round
             if (!(dot(pd, nrm) > 0.0f)) {
                 const float w = GAUSS_ALPHA * (1.0f - (1.0f - pm_expf((-GAUSS_BETA) * dsq / denom)) / GAUSS_DENOM);
-                nf += w * decode_rgbe(__ldg(&g.s_power[k]));
+                nf += w * __ldg(&g.s_pow[k]); // decode_rgbe(s_power[k])
                 found += w;
             }
         }

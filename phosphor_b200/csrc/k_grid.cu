@@ -413,9 +413,13 @@ void launch_radix_sort(const u32 *keys_in, u32 *keys_tmp0, u32 *keys_tmp1, u32 *
 }
 
 // ---- cell-ordered photon records ---------------------------------------------------------------
+// Besides the packed records, each photon's direction and power are decoded here once per round
+// (the same decode_oct / decode_rgbe the gather would apply per pixel and photon), so the gather's
+// per-pixel branch only loads them.
 __global__ void __launch_bounds__(256) k_sorted_records(const u32 *__restrict__ perm, const float4 *__restrict__ ph_pos,
                                                        const uint2 *__restrict__ ph_pd, const u32 *n_dev,
                                                        float4 *__restrict__ s_posdir, u32 *__restrict__ s_power,
+                                                       float4 *__restrict__ s_dir, float4 *__restrict__ s_pow,
                                                        u64 n_max, u32 *err) {
     u64 p = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (p == 0 && *n_dev == 0)
@@ -427,14 +431,34 @@ __global__ void __launch_bounds__(256) k_sorted_records(const u32 *__restrict__ 
     uint2 pd = ph_pd[i];
     s_posdir[p] = make_float4(pos.x, pos.y, pos.z, __uint_as_float(pd.y));
     s_power[p] = pd.x;
+    s_dir[p] = decode_oct(pd.y);
+    s_pow[p] = decode_rgbe(pd.x);
 }
 
 void launch_sorted_records(const u32 *perm, const float4 *ph_pos, const uint2 *ph_pd, const u32 *n_dev, u64 n_max,
-                           float4 *s_posdir, u32 *s_power, u32 *err, cudaStream_t st) {
+                           float4 *s_posdir, u32 *s_power, float4 *s_dir, float4 *s_pow, u32 *err, cudaStream_t st) {
     if (n_max == 0)
         return;
     k_sorted_records<<<(unsigned)((n_max + 255) / 256), 256, 0, st>>>(perm, ph_pos, ph_pd, n_dev, s_posdir, s_power,
-                                                                    n_max, err);
+                                                                    s_dir, s_pow, n_max, err);
+}
+
+// The decoded direction and power of records written from the host.
+__global__ void __launch_bounds__(256) k_decode_records(const float4 *__restrict__ s_posdir,
+                                                       const u32 *__restrict__ s_power, u64 n,
+                                                       float4 *__restrict__ s_dir, float4 *__restrict__ s_pow) {
+    const u64 p = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n)
+        return;
+    s_dir[p] = decode_oct(__float_as_uint(s_posdir[p].w));
+    s_pow[p] = decode_rgbe(s_power[p]);
+}
+
+void launch_decode_records(const float4 *s_posdir, const u32 *s_power, u64 n, float4 *s_dir, float4 *s_pow,
+                           cudaStream_t st) {
+    if (n == 0)
+        return;
+    k_decode_records<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(s_posdir, s_power, n, s_dir, s_pow);
 }
 
 // ---- allocation-free exclusive scan --------------------------------------------------------------

@@ -82,12 +82,15 @@ void launch_radix_sort(const u32 *keys_in, u32 *keys_tmp0, u32 *keys_tmp1, u32 *
                        const u32 *n_dev, u64 n_max, u32 key_bits, void *scratch, u32 *err, cudaStream_t st);
 
 void launch_sorted_records(const u32 *perm, const float4 *ph_pos, const uint2 *ph_pd, const u32 *n_dev, u64 n_max,
-                           float4 *s_posdir, u32 *s_power, u32 *err, cudaStream_t st);
+                           float4 *s_posdir, u32 *s_power, float4 *s_dir, float4 *s_pow, u32 *err, cudaStream_t st);
+void launch_decode_records(const float4 *s_posdir, const u32 *s_power, u64 n, float4 *s_dir, float4 *s_pow,
+                           cudaStream_t st);
 
 struct GatherBufs {
     const float4 *hp_pos, *hp_normal, *hp_throughput, *hp_base_color, *hp_direct, *hp_emission;
     const float4 *s_posdir;
     const u32 *s_power;
+    const float4 *s_dir, *s_pow; // per record: decode_oct(direction bits), decode_rgbe(power)
     const u32 *cell_start; // total_cells+1
     u32 n_cap;             // photon buffer capacity: cell ranges are clamped to it
     float4 *flux;
