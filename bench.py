@@ -199,7 +199,9 @@ def algorithmic_bytes(stage: str, P: int, Ne: int, Ns: int, C: int, scene_bytes:
         "hash": 16 * Ns + 4 * Ns + 4 * C + 8 * Ns,
         "cell_scan": 8 * C,
         "sort": 28 * Ns + 24 * Ns,
-        "records": 0,
+        # permutation (4 B) and canonical photon (24 B) read; packed record, power word and the
+        # decoded direction and power (52 B) written
+        "records": 80 * Ns,
         "gather": 168 * P + 24 * Ns + 8 * C,
     }[stage]
 
