@@ -20,6 +20,8 @@
 // of its own 64-entry stack.
 #pragma once
 
+#include <type_traits>
+
 #include "dev_common.cuh"
 
 namespace phx {
@@ -184,15 +186,68 @@ PHX_DI void sort2(float &ta, i32 &ra, float &tb, i32 &rb) {
     }
 }
 
+// The hits of a ray on [t_min, t_max] that one traversal collects for a shadow ray crossing
+// transmissive surfaces: the K first in the order of (t ascending, reference leaf rank descending)
+// — the order in which closest-hit queries with a rising t_min return them.  Every hit with
+// t <= bound and t < lost is listed: bound is the final culling distance (the K-th listed t once
+// the list is full, or the nearest opaque hit), lost the smallest t of a hit that did not fit.
+template <int K> struct HitList {
+    float t[K], u[K], v[K];
+    i32 tri[K], rank[K];
+    int n;
+    float lost, bound;
+};
+struct NoHitList {};
+template <int K> constexpr int list_capacity(const HitList<K> *) { return K; }
+constexpr int list_capacity(const NoHitList *) { return 0; }
+
+template <int K> PHX_DI void hit_list_insert(HitList<K> &L, float t, float u, float v, i32 tri, i32 rank) {
+    auto before = [&](int i) { return t < L.t[i] || (t == L.t[i] && rank > L.rank[i]); };
+    if (L.n == K) {
+        if (!before(K - 1)) { // sorts after the whole list: dropped
+            L.lost = fminf(L.lost, t);
+            return;
+        }
+        L.lost = fminf(L.lost, L.t[K - 1]); // the last entry makes room
+    }
+    bool placed = false;
+#pragma unroll
+    for (int i = K - 1; i >= 0; i--) {
+        if (placed)
+            continue;
+        if (i > 0 && i - 1 < L.n && before(i - 1)) { // shift the entry after the new hit
+            L.t[i] = L.t[i - 1];
+            L.u[i] = L.u[i - 1];
+            L.v[i] = L.v[i - 1];
+            L.tri[i] = L.tri[i - 1];
+            L.rank[i] = L.rank[i - 1];
+        } else if (i <= L.n) {
+            L.t[i] = t;
+            L.u[i] = u;
+            L.v[i] = v;
+            L.tri[i] = tri;
+            L.rank[i] = rank;
+            placed = true;
+        }
+    }
+    if (L.n < K)
+        L.n++;
+}
+
 // Closest hit in [t_min, t_max] (scene_intersect, hit.h:135-172).  Returns false on a miss.
 // `any` stops at the first accepted hit (only valid where the caller needs no specific hit).
+// With a HitList (LIST), every accepted hit is offered to the list instead and the culling
+// distance follows the list's bound; the return value is then meaningless.
 //
 // Warp-synchronous single-step loop: the lanes that call intersect together stay in lockstep,
 // each iteration advancing every unfinished lane by exactly one node (an inner child pair or a
 // leaf), so neighbouring rays share every node fetch and the warp never runs one lane's inner
 // loop while the others wait.
-PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, float t_max, Hit *hit, u32 *overflow,
-                      bool any = false) {
+template <class LIST>
+PHX_DI bool intersect_t(const SceneDesc &sc, float4 o, float4 d, float t_min, float t_max, Hit *hit, u32 *overflow,
+                        bool any, LIST *list) {
+    constexpr bool LISTED = !std::is_same<LIST, NoHitList>::value;
+    float opaque = t_max; // LISTED: nearest opaque hit so far
     constexpr i32 POP = 0x7fffffff;
     const float ix = 1.0f / d.x, iy = 1.0f / d.y, iz = 1.0f / d.z;
     const float oix = o.x * ix, oiy = o.y * iy, oiz = o.z * iz;
@@ -291,6 +346,15 @@ PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, floa
                 u32 rank;
                 if (tri_test(sc.trirec + 3 * (size_t)(first + k), o.x, o.y, o.z, o.w, d.x, d.y, d.z, d.w, t_min,
                              closest, &t, &u, &v, &rank)) {
+                    if constexpr (LISTED) {
+                        hit_list_insert(*list, t, u, v, (i32)(first + k), (i32)rank);
+                        const u32 mi = __float_as_uint(__ldg(&sc.trirec[3 * (size_t)(first + k)].w));
+                        if (sc.materials[mi].transmission < EPS)
+                            opaque = fminf(opaque, t); // nothing beyond it can be reached
+                        closest = fminf(list->n == list_capacity(list) ? list->t[list_capacity(list) - 1] : t_max,
+                                        opaque);
+                        continue;
+                    }
                     // t <= closest here; at equal t the reference keeps the larger leaf rank
                     if (t < closest || (i32)rank > best_rank) {
                         closest = t;
@@ -317,11 +381,31 @@ PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, floa
             }
         }
     }
+    if constexpr (LISTED) {
+        list->bound = closest;
+        return false;
+    }
     hit->t = closest;
     hit->u = bu;
     hit->v = bv;
     hit->tri = best;
     return best >= 0;
+}
+
+PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, float t_max, Hit *hit, u32 *overflow,
+                      bool any = false) {
+    return intersect_t<NoHitList>(sc, o, d, t_min, t_max, hit, overflow, any, nullptr);
+}
+
+// Collects the hits of (o, d) on [t_min, t_max] into L (see HitList).
+template <int K>
+PHX_DI void intersect_list(const SceneDesc &sc, float4 o, float4 d, float t_min, float t_max, HitList<K> *L,
+                           u32 *overflow) {
+    L->n = 0;
+    L->lost = __int_as_float(0x7f800000);
+    L->bound = t_max;
+    Hit unused;
+    intersect_t<HitList<K>>(sc, o, d, t_min, t_max, &unused, overflow, false, L);
 }
 
 } // namespace phx

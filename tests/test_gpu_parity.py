@@ -365,17 +365,26 @@ def test_image_formation_matches_output_cpp():
 
 
 def _scene_from_arrays(tris, mats, lights, camera):
+    """A scene over caller arrays; the emissive triangle list is the triangle array itself.  The
+    light luminance prefix sum comes from the library's host helper and the UV transforms are zero
+    (no material is textured), as the oracle reads both."""
     sc = A.Scene()
     sc.triangles = tris.ctypes.data_as(C.POINTER(A.Triangle))
     sc.n_triangles = len(tris)
     sc.materials = mats.ctypes.data_as(C.POINTER(A.Material))
     sc.n_materials = len(mats)
+    uv = (A.UvTransformBlock * len(mats))()
+    sc.uv_transforms = C.cast(uv, C.POINTER(A.UvTransformBlock))
     sc.emissive_triangles = tris.ctypes.data_as(C.POINTER(A.Triangle))
     sc.n_emissive_triangles = len(tris)
     sc.lights = lights.ctypes.data_as(C.POINTER(A.Light))
     sc.n_lights = len(lights)
+    lum = np.zeros(max(len(lights), 1), np.float32)
+    A.check(A.load().phx_lum_pref_sum(lights.ctypes.data_as(C.POINTER(A.Light)), len(lights),
+                                      lum.ctypes.data_as(C.POINTER(C.c_float))))
+    sc.lum_pref_sum = lum.ctypes.data_as(C.POINTER(C.c_float))
     sc.camera = camera
-    return P.SceneData(sc, keep=(tris, mats, lights))
+    return P.SceneData(sc, keep=(tris, mats, lights, uv, lum))
 
 
 def test_no_photon_hit_is_a_status():
@@ -403,6 +412,56 @@ def test_no_photon_hit_is_a_status():
         with pytest.raises(P.PhxError) as e:
             r.emit_photons(5)
         assert e.value.code == A.PHX_E_NO_PHOTONS
+
+
+def _glass_panes_scene():
+    """The Cornell box with three horizontal transmissive panes between the floor and the ceiling
+    light: shadow rays from the floor cross three surfaces."""
+    base = P.SceneData.generate(A.PHX_SCENE_CORNELL, seed=1, width=32, height=32)
+    box = base.triangles().copy()
+    panes = np.zeros(6, dtype=box.dtype)
+    for q, y in enumerate((0.25, 0.5, 0.75)):
+        corners = [(0.1, 0.1), (0.9, 0.1), (0.9, 0.9), (0.1, 0.9)]
+        for k, tri in enumerate(((0, 1, 2), (0, 2, 3))):
+            p = panes[2 * q + k]
+            for v, c in zip(("v0", "v1", "v2"), tri):
+                p[v]["x"], p[v]["y"], p[v]["z"] = corners[c][0], y, corners[c][1]
+            for n in ("n0", "n1", "n2"):
+                p[n]["y"] = 1.0
+            p["mat_index"] = 4
+    tris = np.concatenate([box, panes])
+    mats = np.concatenate([base.materials(), base.materials()[:1]]).copy()
+    glass = mats[4]
+    glass["transmission"], glass["roughness"], glass["ior"] = 1.0, 0.1, 1.5
+    glass["base_color"]["x"], glass["base_color"]["y"], glass["base_color"]["z"] = 0.9, 0.95, 0.9
+    lights = base.lights().copy()
+    light_tris = np.flatnonzero(tris["mat_index"] == 3)
+    aux = np.array([lights[0]["aux"][c] for c in "xyzw"], np.float32).view(np.uint32)
+    aux[1], aux[2] = light_tris[0], len(light_tris)  # emissive range within the triangle array
+    for c, v in zip("xyzw", aux.view(np.float32)):
+        lights[0]["aux"][c] = v
+    return _scene_from_arrays(tris, mats, lights, base.scene.camera)
+
+
+def test_shadow_rays_through_several_transmissive_surfaces():
+    """Shadow rays that cross more transmissive surfaces than one traversal lists go on with
+    closest-hit queries past the listed ones; hit points (direct light included) stay bit-exact."""
+    scene = _glass_panes_scene()
+    args = P.ArgsList(width=40, height=40, photons_per_round=1 << 12, max_photon_bounces=8, grid_res=16,
+                      direct_samples=16)
+    o = O.Oracle(scene)
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        seed = 0x51ED
+        r.trace_rays(seed)
+        got = np.stack([r.read(b) for b in ["HP_POS", "HP_NORMAL", "HP_THROUGHPUT", "HP_BASE_COLOR", "HP_DIRECT",
+                                             "HP_EMISSION"]], axis=1)
+        r.iterate(2)
+        assert r.info().stack_overflows == 0
+    want = o.trace(args.width, args.height, seed, args.direct_samples)
+    assert assert_close("panes hit points", got, want) == 1.0
+    diffuse = want[:, 5, 3] == 1.0
+    assert diffuse.mean() > 0.3 and (want[diffuse, 4, :3] > 0).any()  # light reaches through the panes
 
 
 def test_state_and_argument_errors():
