@@ -76,6 +76,7 @@ constexpr u32 ERR_LOOKBACK_TIMEOUT = 1u;
 constexpr u32 ERR_STACK_OVERFLOW = 2u;
 constexpr u32 ERR_SLOT_OVERFLOW = 4u;
 constexpr u32 ERR_NO_PHOTONS = 8u;
+constexpr u32 ERR_DEFER_OVERFLOW = 16u; // a deferred emission term did not fit its pixel's list
 
 // ---- float4 ----------------------------------------------------------------------------------
 PHX_HDI float4 f4(float x, float y, float z, float w) { return make_float4(x, y, z, w); }

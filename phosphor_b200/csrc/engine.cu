@@ -59,7 +59,8 @@ Engine::~Engine() {
     for (auto &s : sc)
         for (auto &b : s.bufs)
             b.release();
-    DevBuf *all[] = {&d_desc, &d_pix_bases, &d_emit_bases, &d_nee_bases, &nee_ray, &nee_val, &d_seeds, &d_rng,
+    DevBuf *all[] = {&d_desc, &d_pix_bases, &d_emit_bases, &d_nee_bases, &nee_ray, &nee_val, &spec_ray, &spec_val,
+                     &spec_org, &spec_pix, &spec_next, &def_cnt, &def_prefix, &def_val, &def_tag, &d_seeds, &d_rng,
                      &d_err, &d_ovf, &d_queue, &d_ntotal,
                      &flux, &weight, &radiance, &slot_pos, &slot_pd, &counts, &offsets, &ph_pos, &ph_pd, &keys,
                      &cell_count, &cell_start, &sk0, &sk1, &sv0, &sv1, &s_posdir, &s_power, &s_dir, &s_pow, &scan_scr, &radix_scr,
@@ -355,6 +356,12 @@ int Engine::create(const phx_scene *scenes, const phx_params *params, uint32_t n
     if ((r = upload(d_desc, descs.data(), sizeof(SceneDesc) * n)) || (r = upload(d_pix_bases, pb.data(), 4 * pb.size())) ||
         (r = upload(d_emit_bases, eb.data(), 4 * eb.size())) || (r = upload(d_nee_bases, nb.data(), 4 * nb.size())) ||
         (r = nee_ray.alloc(16 * (size_t)total_nee)) || (r = nee_val.alloc(16 * (size_t)total_nee)) ||
+        (r = spec_ray.alloc(16 * (size_t)total_nee)) || (r = spec_val.alloc(16 * (size_t)total_nee)) ||
+        (r = spec_org.alloc(16 * (size_t)total_nee)) || (r = spec_pix.alloc(4 * (size_t)total_nee)) ||
+        (r = upload(spec_next, nullptr, 16)) || (r = upload(def_cnt, nullptr, 4 * (size_t)total_pixels)) ||
+        (r = def_prefix.alloc(16 * (size_t)total_pixels)) ||
+        (r = def_val.alloc(16 * (size_t)DEF_MAX * total_pixels)) ||
+        (r = def_tag.alloc(4 * (size_t)DEF_MAX * total_pixels)) ||
         (r = upload(d_rng, rng.data(), 4 * n)) ||
         (r = upload(d_seeds, nullptr, 4 * n)) || (r = upload(d_err, nullptr, 16)) || (r = upload(d_ovf, nullptr, 16)) ||
         (r = upload(d_queue, nullptr, 16)) || (r = upload(d_ntotal, nullptr, 16)))
@@ -460,12 +467,30 @@ void Engine::enq_trace() {
     TraceOut o{hp[0].as<float4>(), hp[1].as<float4>(), hp[2].as<float4>(), hp[3].as<float4>(),
                hp[4].as<float4>(), hp[5].as<float4>(), nee_ray.as<float4>(), nee_val.as<float4>()};
     const LaunchCtx l = lc();
+    const bool spec = spec_deferred();
+    if (spec) {
+        o.spec_ray = spec_ray.as<float4>();
+        o.spec_val = spec_val.as<float4>();
+        o.spec_org = spec_org.as<float4>();
+        o.spec_pix = spec_pix.as<u32>();
+        o.spec_next = spec_next.as<u32>();
+        o.spec_cap = total_nee;
+        o.def_cnt = def_cnt.as<u32>();
+        o.def_prefix = def_prefix.as<float4>();
+        o.def_val = def_val.as<float4>();
+        o.def_tag = def_tag.as<u32>();
+        cudaMemsetAsync(spec_next.p, 0, sizeof(u32), st);
+    }
     launch_trace(l, o, (int)tune.trace_block, (int)tune.persistent, (int)tune.trace_blocks_per_sm, d_queue.as<u32>(),
                  st);
     ev(ST_TRACE, true);
     ev(ST_SHADOW, false);
     launch_shadow(l, o, (int)tune.trace_block, st);
+    if (spec)
+        launch_spec_shadow(l, o, (int)tune.trace_blocks_per_sm, st);
     launch_nee_resolve(l, o, st);
+    if (spec)
+        launch_spec_resolve(l, o, st);
     ev(ST_SHADOW, true);
     stage_state |= 1;
 }
@@ -588,6 +613,8 @@ int Engine::sync_and_check() {
         return fail(PHX_E_TIMEOUT, "a decoupled look-back wait gave up (device error flag set)");
     if (err & ERR_NO_PHOTONS)
         return fail(PHX_E_NO_PHOTONS, "no photon was stored in a round (renderer.cpp:117-118)");
+    if (err & ERR_DEFER_OVERFLOW)
+        return fail(PHX_E_STATE, "a deferred specular emission term did not fit its pixel's list");
     return PHX_OK;
 }
 
@@ -1150,7 +1177,8 @@ int Engine::info(uint32_t s, phx_info *o) {
     o->trav_inner_nodes = S.trav_inner;
     // seeds, trace, [shadow, resolve], emit, count scan, compaction, hash, cell scan, 3 per sort
     // pass, records, gather
-    o->kernels_per_round = 9 + 3 * o->sort_passes + (tune.nee_wavefront ? 3 : 0) +
+    // (+2 with the specular NEE deferred: its shadow kernel and its resolve)
+    o->kernels_per_round = 9 + 3 * o->sort_passes + (tune.nee_wavefront ? 3 : 0) + (spec_deferred() ? 2 : 0) +
                            (tune.gather_sorted && pix_key_bits ? 1 + 3 * radix_passes(pix_key_bits) : 0);
     CK(cudaStreamSynchronize(st));
     uint32_t v[2] = {0, 0};

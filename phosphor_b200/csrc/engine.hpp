@@ -142,6 +142,9 @@ class Engine {
 
     DevBuf d_desc, d_pix_bases, d_emit_bases, d_nee_bases, d_seeds, d_rng, d_err, d_ovf, d_queue, d_ntotal;
     DevBuf nee_ray, nee_val;
+    // deferred specular NEE: sample slots (as many as the diffuse ones) and per-pixel term lists
+    DevBuf spec_ray, spec_val, spec_org, spec_pix, spec_next, def_cnt, def_prefix, def_val, def_tag;
+    bool spec_deferred() const { return tune.persistent && tune.nee_wavefront && total_nee > 0; }
     DevBuf hp[6], flux, weight, radiance;
     DevBuf slot_pos, slot_pd, counts, offsets, ph_pos, ph_pd, keys, cell_count, cell_start;
     DevBuf sk0, sk1, sv0, sv1, s_posdir, s_power, s_dir, s_pow, scan_scr, radix_scr, img_rgb, img_ldr;

@@ -196,9 +196,35 @@ struct CameraPath {
     // pending shadow query (shadow_transmittance, light_sampling.h:302-333)
     float4 m, trans;
     u32 sh_depth;
+    u32 def_n; // emission terms listed for the deferred specular NEE (0: none deferred yet)
 };
 
+// Adds one term to the path's emission.  Once the path has deferred a specular NEE term, the sum
+// is completed after the shadow pass (k_spec_resolve), so its later terms are listed in order
+// instead.  A zero term is left out: the sum starts at +0 and only ever adds, so it is never -0 and
+// e + (+-0) == e bit for bit.
+PHX_DI void cp_add_emission(CameraPath &p, const TraceOut &out, float4 a) {
+    if (p.def_n == 0) {
+        p.emission += a;
+        return;
+    }
+    if (a.x == 0.0f && a.y == 0.0f && a.z == 0.0f && a.w == 0.0f)
+        return;
+    if (p.def_n >= DEF_MAX) { // cannot happen (at most 10 terms follow a deferred one); reported
+        p.def_n |= DEF_OVERFLOW;
+        return;
+    }
+    const size_t k = (size_t)p.gpix * DEF_MAX + p.def_n++;
+    out.def_val[k] = a;
+    out.def_tag[k] = DEF_KNOWN;
+}
+
 PHX_DI void cp_finish(CameraPath &p, const TraceOut &out, bool diffuse_hit, bool deferred = false) {
+    if (out.def_cnt) {
+        out.def_cnt[p.gpix] = p.def_n | (diffuse_hit ? DEF_DIFFUSE : 0u);
+        if (p.def_n)
+            out.def_prefix[p.gpix] = p.emission;
+    }
     TraceResult r;
     r.throughput = p.throughput;
     if (diffuse_hit) {
@@ -226,11 +252,35 @@ PHX_DI void cp_start(CameraPath &p, const SceneDesc *sc, u32 seed, u32 tid, u32 
     make_ray(sc->camera, tid % sc->width, tid / sc->width, sc->width, sc->height, &p.rng, &p.origin, &p.dir);
     p.throughput = white4();
     p.emission = zero4();
+    p.def_n = 0;
     init_ior_stack(&p.ior, AIR_IOR);
     p.depth = 0;
     p.phase = PH_CAMERA;
     p.t_min = EPS;
     p.t_max = INF;
+}
+
+// One sample of direct_lighting_specular (light_sampling.h:355-390) up to its shadow query: false
+// when it contributes nothing (no RNG draw depends on a shadow query's outcome), else the light
+// fragment and the weight m of its transmittance.
+PHX_DI bool spec_sample(CameraPath &p, LightFragment *f, float4 *m) {
+    const SceneDesc &sc = *p.sc;
+    float ndv = dot(p.view, p.sn);
+    if (ndv < EPS)
+        return false;
+    if (!sample_light_fragment(&p.rng, sc, p.pos, p.sn, f) || f->n_dot_dir < EPS)
+        return false;
+    float alpha = p.rough * p.rough;
+    float4 h = normalize(f->dir + p.view);
+    float ndh = fmaxf(dot(p.sn, h), 0.0f);
+    float g = ggx_ndf(ndh, alpha);
+    float4 fr = fresnel4(p.f0, p.view, h);
+    float sm = smith_g1_ggx(f->n_dot_dir, alpha) * smith_g1_ggx(ndv, alpha);
+    float4 spec = f->radiance * g * fr * sm / (4.0f * f->n_dot_dir * ndv);
+    if (dot(spec, spec) < EPS * EPS)
+        return false;
+    *m = spec;
+    return true;
 }
 
 // Runs the NEE loop from sample nee_i until a shadow query is needed (returns true with the query
@@ -248,32 +298,13 @@ PHX_DI bool cp_next_shadow(CameraPath &p) {
             p.m = f.radiance * (p.base / PI);
             p.dir = f.dir;
             p.t_max = f.dist - EPS;
-        } else { // direct_lighting_specular, light_sampling.h:355-390
-            float ndv = dot(p.view, p.sn);
-            if (ndv < EPS) {
-                p.nee_sum += zero4();
-                p.nee_i++;
-                continue;
-            }
+        } else {
             LightFragment f;
-            if (!sample_light_fragment(&p.rng, sc, p.pos, p.sn, &f) || f.n_dot_dir < EPS) {
+            if (!spec_sample(p, &f, &p.m)) {
                 p.nee_sum += zero4();
                 p.nee_i++;
                 continue;
             }
-            float alpha = p.rough * p.rough;
-            float4 h = normalize(f.dir + p.view);
-            float ndh = fmaxf(dot(p.sn, h), 0.0f);
-            float g = ggx_ndf(ndh, alpha);
-            float4 fr = fresnel4(p.f0, p.view, h);
-            float sm = smith_g1_ggx(f.n_dot_dir, alpha) * smith_g1_ggx(ndv, alpha);
-            float4 spec = f.radiance * g * fr * sm / (4.0f * f.n_dot_dir * ndv);
-            if (dot(spec, spec) < EPS * EPS) {
-                p.nee_sum += zero4();
-                p.nee_i++;
-                continue;
-            }
-            p.m = spec;
             p.dir = f.dir;
             p.t_max = f.dist - EPS;
         }
@@ -321,8 +352,62 @@ PHX_DI bool cp_after_nee(CameraPath &p, const TraceOut &out) {
         return false;
     }
     if (p.nee_kind == NEE_SPECULAR)
-        p.emission += p.throughput * (p.nee_sum / (float)p.sc->direct_samples);
+        cp_add_emission(p, out, p.throughput * (p.nee_sum / (float)p.sc->direct_samples));
     return cp_continue(p, out);
+}
+
+// Claims n consecutive slots of a counter for each calling lane; the converged lanes asking for the
+// same n share one atomic.
+PHX_DI u32 claim_slots(u32 *counter, u32 n) {
+    const u32 lane = threadIdx.x & 31u;
+    const u32 same = __match_any_sync(__activemask(), n);
+    const u32 leader = __ffs(same) - 1;
+    u32 base = 0;
+    if (lane == leader)
+        base = atomicAdd(counter, n * (u32)__popc(same));
+    base = __shfl_sync(same, base, leader);
+    return base + n * (u32)__popc(same & ((1u << lane) - 1u));
+}
+
+// Specular NEE without the shadow queries: draws the event's samples in order (the path's RNG
+// advances exactly as in the traced form), records each shadow ray with its weight in claimed
+// sample slots and lists the NEE term (throughput * mean of the samples' contributions) for
+// k_spec_resolve.  Returns false, having changed nothing, when the sample slots are exhausted.
+// Out of line: it runs once per specular event and would otherwise add its registers to every
+// step of the camera kernel's loop.
+static __device__ __noinline__ bool cp_defer_specular(CameraPath &p, const TraceOut &out) {
+    const u32 ds = p.sc->direct_samples;
+    if (p.def_n >= DEF_MAX)
+        return false;
+    const u32 base = claim_slots(out.spec_next, ds);
+    if (ds > out.spec_cap || base > out.spec_cap - ds) {
+        // no room: the slots of this claim that lie below the capacity carry no ray
+        for (u32 slot = base; slot < out.spec_cap && slot - base < ds; slot++) {
+            out.spec_ray[slot] = f4(0.0f, 0.0f, 0.0f, -1.0f);
+            out.spec_val[slot] = zero4();
+            out.spec_org[slot] = zero4();
+            out.spec_pix[slot] = p.gpix;
+        }
+        return false;
+    }
+    for (u32 i = 0; i < ds; i++) {
+        LightFragment f;
+        float4 m;
+        const u32 slot = base + i;
+        if (spec_sample(p, &f, &m)) {
+            out.spec_ray[slot] = f4(f.dir.x, f.dir.y, f.dir.z, f.dist);
+            out.spec_val[slot] = m;
+        } else {
+            out.spec_ray[slot] = f4(0.0f, 0.0f, 0.0f, -1.0f);
+            out.spec_val[slot] = zero4();
+        }
+        out.spec_org[slot] = p.pos;
+        out.spec_pix[slot] = p.gpix;
+    }
+    const size_t k = (size_t)p.gpix * DEF_MAX + p.def_n++;
+    out.def_val[k] = p.throughput;
+    out.def_tag[k] = base;
+    return true;
 }
 
 // Consumes the result of the pending query; returns true while the path needs another query.
@@ -373,7 +458,7 @@ PHX_DI bool cp_advance(CameraPath &p, bool hit, const Hit &h, const TraceOut &ou
     // camera query (trace_rays.cl:64-147)
     if (!hit) {
         if (sc.has_env)
-            p.emission += p.throughput * sample_envmap(sc, p.dir);
+            cp_add_emission(p, out, p.throughput * sample_envmap(sc, p.dir));
         cp_finish(p, out, false);
         return false;
     }
@@ -385,7 +470,7 @@ PHX_DI bool cp_advance(CameraPath &p, bool hit, const Hit &h, const TraceOut &ou
     float4 tangent, bitangent;
     hit_frame(sc, h, sh, &tangent, &bitangent);
     ShadingContext ctx = evaluate_material(sc, mat, sh.mat_index, sh.uvx, sh.uvy, sh.normal, tangent, bitangent);
-    p.emission += p.throughput * ctx.emissive;
+    cp_add_emission(p, out, p.throughput * ctx.emissive);
     p.view = -p.dir;
     BsdfSample bs = sample_bsdf(&p.rng, ctx, ctx.shading_normal, sh.normal, p.view, &p.ior, sh.front_face);
     p.pos = sh.position;
@@ -417,6 +502,8 @@ PHX_DI bool cp_advance(CameraPath &p, bool hit, const Hit &h, const TraceOut &ou
         p.nee_kind = NEE_NONE;
         return cp_continue(p, out);
     }
+    if (defer && out.spec_ray && cp_defer_specular(p, out))
+        return cp_continue(p, out);
     if (cp_next_shadow(p))
         return true;
     return cp_after_nee(p, out);
@@ -492,6 +579,76 @@ __global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow(LaunchCtx lc, T
             atomicAdd(lc.overflow, ovf);
     }
     out.nee_val[g] = contrib;
+}
+
+// Deferred specular NEE samples: one thread per claimed sample slot.  An event's samples are
+// consecutive, so a warp traces rays from one or two hit points toward the lights together.  The
+// contribution is the traced form's: weight * transmittance, zero for a sample without a ray.
+__global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow_spec(LaunchCtx lc, TraceOut out) {
+    const u32 n = min(*out.spec_next, out.spec_cap);
+    u32 ovf = 0;
+    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
+        const float4 ray = out.spec_ray[g];
+        if (ray.w < 0.0f) {
+            out.spec_val[g] = zero4();
+            continue;
+        }
+        const u32 gpix = out.spec_pix[g];
+        const SceneDesc &sc = lc.scenes[lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gpix)];
+        const float4 trans = shadow_transmittance(sc, out.spec_org[g], f4(ray.x, ray.y, ray.z, 0.0f), ray.w, &ovf);
+        out.spec_val[g] = out.spec_val[g] * trans;
+    }
+    if (ovf)
+        atomicAdd(lc.overflow, ovf);
+}
+
+// Completes the emission of every pixel that deferred a specular NEE term: its listed terms are
+// added to the prefix in path order, an NEE term as throughput * (sum of its samples in sample
+// order / direct_samples) — the traced form's float operations, in the same order.
+__global__ void __launch_bounds__(256) k_spec_resolve(LaunchCtx lc, TraceOut out) {
+    const u32 gpix = lc.pix_lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (gpix >= lc.pix_hi)
+        return;
+    const SceneDesc &sc = lc.scenes[lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gpix)];
+    if (!sc.active)
+        return;
+    const u32 c = out.def_cnt[gpix];
+    if (c & DEF_OVERFLOW) {
+        atomicOr(lc.err, ERR_DEFER_OVERFLOW);
+        return;
+    }
+    const u32 n = c & 0xffu;
+    if (n == 0)
+        return;
+    const u32 ds = sc.direct_samples;
+    float4 e = out.def_prefix[gpix];
+    for (u32 i = 0; i < n; i++) {
+        const size_t k = (size_t)gpix * DEF_MAX + i;
+        const u32 tag = out.def_tag[k];
+        const float4 v = out.def_val[k];
+        if (tag == DEF_KNOWN) {
+            e += v;
+            continue;
+        }
+        float4 sum = zero4();
+        for (u32 j = 0; j < ds; j++)
+            sum += out.spec_val[tag + j];
+        e += v * (sum / (float)ds);
+    }
+    out.emission[gpix] = (c & DEF_DIFFUSE) ? f4(e.x, e.y, e.z, 1.0f) : e;
+}
+
+void launch_spec_shadow(const LaunchCtx &lc, const TraceOut &out, int blocks_per_sm, cudaStream_t st) {
+    if (!out.spec_ray || out.spec_cap == 0)
+        return;
+    const int grid = g_sm_count * (blocks_per_sm > 0 ? blocks_per_sm : 8);
+    k_shadow_spec<<<grid, 128, 0, st>>>(lc, out);
+}
+
+void launch_spec_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st) {
+    if (!out.def_cnt || lc.pix_hi <= lc.pix_lo)
+        return;
+    k_spec_resolve<<<(lc.pix_hi - lc.pix_lo + 255) / 256, 256, 0, st>>>(lc, out);
 }
 
 // Sums each pixel's samples in sample order (trace_rays.cl:104-118).

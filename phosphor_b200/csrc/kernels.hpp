@@ -28,10 +28,30 @@ struct LaunchCtx {
     u32 emit_lo, emit_hi;    // global photon paths the photon pass emits
 };
 
+// Deferred specular NEE: per pixel at most two emission terms per camera bounce (the surface's
+// emission, the NEE mean) and one for an escaped ray.
+constexpr u32 DEF_MAX = 11;
+constexpr u32 DEF_KNOWN = 0xffffffffu; // def_tag of a term whose value is known
+constexpr u32 DEF_DIFFUSE = 0x100u;    // def_cnt flag: the path ended at a diffuse hit point
+constexpr u32 DEF_OVERFLOW = 0x40000000u; // def_cnt flag: a term did not fit (never expected)
+
 struct TraceOut {
     float4 *pos, *normal, *throughput, *base_color, *direct, *emission;
     float4 *nee_ray; // per NEE sample slot: (dir.xyz, light distance), w < 0 = no contribution
     float4 *nee_val; // per slot: radiance * (base / pi); replaced by the contribution in the shadow pass
+    // Deferred specular NEE (lane-refill camera kernel; null: traced in place).  Each specular
+    // event claims direct_samples consecutive sample slots; from a pixel's first deferred event on,
+    // its nonzero emission terms are listed in order and summed once the samples are traced.
+    float4 *spec_ray = nullptr; // per sample: (dir.xyz, light distance), w < 0 = no contribution
+    float4 *spec_val = nullptr; // per sample: the NEE weight; replaced by weight * transmittance
+    float4 *spec_org = nullptr; // per sample: shadow ray origin (the specular hit point)
+    u32 *spec_pix = nullptr;    // per sample: global pixel (its scene)
+    u32 *spec_next = nullptr;   // claimed sample slots this round (zeroed before the camera pass)
+    u32 spec_cap = 0;           // sample slots
+    u32 *def_cnt = nullptr;     // per pixel: listed terms | DEF_DIFFUSE
+    float4 *def_prefix = nullptr; // per pixel: the emission before its first listed term
+    float4 *def_val = nullptr;  // per pixel x DEF_MAX: a known term, or the throughput of an NEE term
+    u32 *def_tag = nullptr;     // per pixel x DEF_MAX: DEF_KNOWN, or the first sample slot of an NEE term
 };
 
 // Persistent work queue (lane refill): a device counter the kernel drains.
@@ -41,6 +61,9 @@ void launch_trace(const LaunchCtx &lc, const TraceOut &out, int block, int persi
 // each pixel's samples in sample order into hp_direct.
 void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int block, cudaStream_t st);
 void launch_nee_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st);
+// Deferred specular NEE: trace the claimed sample slots, then complete each listed pixel's emission.
+void launch_spec_shadow(const LaunchCtx &lc, const TraceOut &out, int blocks_per_sm, cudaStream_t st);
+void launch_spec_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st);
 
 struct EmitOut {
     float4 *slot_pos;
