@@ -21,7 +21,9 @@ struct SurfaceHit {
 PHX_DI u32 tri_mat(const SceneDesc &sc, i32 tri) { return __float_as_uint(__ldg(&sc.trirec[3 * (size_t)tri].w)); }
 
 // hit.h:174-197 (compute_bary hit.h:31-43)
-PHX_SHADE_HIT SurfaceHit process_hit(const SceneDesc &sc, const Hit &h, float4 origin, float4 dir) {
+// The texture coordinates are interpolated only when need_uv (they feed texture lookups alone).
+PHX_SHADE_HIT SurfaceHit process_hit(const SceneDesc &sc, const Hit &h, float4 origin, float4 dir,
+                                     bool need_uv = true) {
     SurfaceHit s;
     s.t = h.t;
     s.tri = h.tri;
@@ -38,11 +40,21 @@ PHX_SHADE_HIT SurfaceHit process_hit(const SceneDesc &sc, const Hit &h, float4 o
     bool front = dot(dir, outward) < 0.0f;
     s.normal = front ? outward : -outward;
     s.front_face = front;
-    const float4 *uv = sc.tri_uv + 2 * (size_t)h.tri;
-    float4 uva = __ldg(uv), uvb = __ldg(uv + 1);
-    s.uvx = w * uva.x + u * uva.z + v * uvb.x;
-    s.uvy = w * uva.y + u * uva.w + v * uvb.y;
+    s.uvx = 0.0f;
+    s.uvy = 0.0f;
+    if (need_uv) {
+        const float4 *uv = sc.tri_uv + 2 * (size_t)h.tri;
+        float4 uva = __ldg(uv), uvb = __ldg(uv + 1);
+        s.uvx = w * uva.x + u * uva.z + v * uvb.x;
+        s.uvy = w * uva.y + u * uva.w + v * uvb.y;
+    }
     return s;
+}
+
+// Whether a material reads any texture (and so the hit's texture coordinates).
+PHX_DI bool mat_textured(const phx_material &m) {
+    return m.diff_index != NO_TEXTURE || m.emis_index != NO_TEXTURE || m.norm_index != NO_TEXTURE ||
+           m.occlusion_index != NO_TEXTURE || m.metal_rough_index != NO_TEXTURE || m.transmission_index != NO_TEXTURE;
 }
 
 // ---- textures: include/common/material.h:66-149 ------------------------------------------------

@@ -40,8 +40,8 @@ PHX_DI u32 emit_path(const SceneDesc &sc, u32 seed, u32 tid, const EmitOut &out,
         bool hit = intersect(sc, origin, dir, EPS, INF, &h, overflow);
         if (!hit)
             return n_out;
-        SurfaceHit sh = process_hit(sc, h, origin, dir);
-        const phx_material mat = sc.materials[sh.mat_index];
+        const phx_material mat = sc.materials[tri_mat(sc, h.tri)];
+        SurfaceHit sh = process_hit(sc, h, origin, dir, mat_textured(mat));
         float4 vol = white4();
         float cur = current_ior(&ior);
         if (cur != AIR_IOR && mat.thickness > EPS && mat.att_dist > EPS) {
@@ -49,8 +49,9 @@ PHX_DI u32 emit_path(const SceneDesc &sc, u32 seed, u32 tid, const EmitOut &out,
             power *= vol;
             throughput *= vol;
         }
-        float4 tangent, bitangent;
-        hit_frame(sc, h, sh, &tangent, &bitangent);
+        float4 tangent = zero4(), bitangent = zero4(); // the frame only serves a normal map
+        if (mat.norm_index != NO_TEXTURE)
+            hit_frame(sc, h, sh, &tangent, &bitangent);
         ShadingContext ctx = evaluate_material(sc, mat, sh.mat_index, sh.uvx, sh.uvy, sh.normal, tangent, bitangent);
         if (depth >= RR_MIN_PHOTON_DEPTH) {
             float q = fmaxf(throughput.x, fmaxf(throughput.y, throughput.z));
@@ -125,16 +126,17 @@ PHX_DI bool pp_advance(PhotonPath &p, bool hit, const Hit &h, const EmitOut &out
     const SceneDesc &sc = *p.sc;
     if (!hit)
         return false;
-    SurfaceHit sh = process_hit(sc, h, p.origin, p.dir);
-    const phx_material mat = sc.materials[sh.mat_index];
+    const phx_material mat = sc.materials[tri_mat(sc, h.tri)];
+    SurfaceHit sh = process_hit(sc, h, p.origin, p.dir, mat_textured(mat));
     float cur = current_ior(&p.ior);
     if (cur != AIR_IOR && mat.thickness > EPS && mat.att_dist > EPS) {
         float4 vol = beer_lambert(f4(mat.att_color), mat.att_dist, sh.t);
         p.power *= vol;
         p.throughput *= vol;
     }
-    float4 tangent, bitangent;
-    hit_frame(sc, h, sh, &tangent, &bitangent);
+    float4 tangent = zero4(), bitangent = zero4(); // the frame only serves a normal map
+    if (mat.norm_index != NO_TEXTURE)
+        hit_frame(sc, h, sh, &tangent, &bitangent);
     ShadingContext ctx = evaluate_material(sc, mat, sh.mat_index, sh.uvx, sh.uvy, sh.normal, tangent, bitangent);
     if (p.depth >= RR_MIN_PHOTON_DEPTH) {
         float q = fmaxf(p.throughput.x, fmaxf(p.throughput.y, p.throughput.z));

@@ -99,16 +99,17 @@ PHX_DI void trace_pixel(const SceneDesc &sc, u32 seed, u32 tid, const TraceOut &
                 emission += throughput * sample_envmap(sc, dir);
             break;
         }
-        SurfaceHit sh = process_hit(sc, h, origin, dir);
-        const phx_material mat = sc.materials[sh.mat_index];
+        const phx_material mat = sc.materials[tri_mat(sc, h.tri)];
+        SurfaceHit sh = process_hit(sc, h, origin, dir, mat_textured(mat));
         float4 vol = white4();
         float cur = current_ior(&ior);
         if (cur != AIR_IOR && mat.thickness > EPS && mat.att_dist > EPS) {
             vol = beer_lambert(f4(mat.att_color), mat.att_dist, sh.t);
             throughput *= vol;
         }
-        float4 tangent, bitangent;
-        hit_frame(sc, h, sh, &tangent, &bitangent);
+        float4 tangent = zero4(), bitangent = zero4(); // the frame only serves a normal map
+        if (mat.norm_index != NO_TEXTURE)
+            hit_frame(sc, h, sh, &tangent, &bitangent);
         ShadingContext ctx = evaluate_material(sc, mat, sh.mat_index, sh.uvx, sh.uvy, sh.normal, tangent, bitangent);
         emission += throughput * ctx.emissive;
         float4 view = -dir;
@@ -462,13 +463,14 @@ PHX_DI bool cp_advance(CameraPath &p, bool hit, const Hit &h, const TraceOut &ou
         cp_finish(p, out, false);
         return false;
     }
-    SurfaceHit sh = process_hit(sc, h, p.origin, p.dir);
-    const phx_material mat = sc.materials[sh.mat_index];
+    const phx_material mat = sc.materials[tri_mat(sc, h.tri)];
+    SurfaceHit sh = process_hit(sc, h, p.origin, p.dir, mat_textured(mat));
     float cur = current_ior(&p.ior);
     if (cur != AIR_IOR && mat.thickness > EPS && mat.att_dist > EPS)
         p.throughput *= beer_lambert(f4(mat.att_color), mat.att_dist, sh.t);
-    float4 tangent, bitangent;
-    hit_frame(sc, h, sh, &tangent, &bitangent);
+    float4 tangent = zero4(), bitangent = zero4(); // the frame only serves a normal map
+    if (mat.norm_index != NO_TEXTURE)
+        hit_frame(sc, h, sh, &tangent, &bitangent);
     ShadingContext ctx = evaluate_material(sc, mat, sh.mat_index, sh.uvx, sh.uvy, sh.normal, tangent, bitangent);
     cp_add_emission(p, out, p.throughput * ctx.emissive);
     p.view = -p.dir;
