@@ -50,9 +50,10 @@ CONFIGS = {
 METRIC = "Mphotons/s"
 # dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu capture of the full-size
 # workload (profiles/dram_traffic_caustic_1024.md)
-# (the shadow stage: k_nee_sample + k_shadow; k_nee_resolve, under 5 % of the stage, not captured)
-NCU_TRAFFIC = {"caustic": {"trace": 1_329_052_672, "shadow": 1_608_642_560, "emit": 506_128_640,
-                           "gather": 225_226_240}}
+# (a stage's kernels summed; the shadow stage: k_nee_sample, k_shadow, k_shadow_spec, k_nee_resolve,
+# k_spec_resolve)
+NCU_TRAFFIC = {"caustic": {"trace": 1_355_299_328, "shadow": 2_066_197_504, "emit": 383_891_200,
+                           "gather": 290_075_136}}
 ALGO_STAGES = ["trace", "shadow", "emit", "emit_scan", "hash", "cell_scan", "sort", "records", "gather"]
 
 
@@ -186,14 +187,18 @@ def run_reference(a, cfg: dict) -> dict:
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
-def algorithmic_bytes(stage: str, P: int, Ne: int, Ns: int, C: int, scene_bytes: int, ds: int = 16) -> int:
+def algorithmic_bytes(stage: str, P: int, Ne: int, Ns: int, C: int, scene_bytes: int, ds: int = 16,
+                      S: int = 0) -> int:
     """Compulsory bytes per round of each stage: the hit-point, photon, cell and image records each
-    stage must read or write once, plus the scene geometry for the traversal stages."""
+    stage must read or write once, plus the scene geometry for the traversal stages.  S = specular
+    NEE samples the camera pass deferred."""
     return {
-        # camera pass: the hit point (96 B) and the NEE stash (32 B) per pixel
-        "trace": 96 * P + 32 * P + scene_bytes,
-        # NEE samples written (32 B), read and replaced by the shadow pass (32 + 16 B), summed (16 B)
-        "shadow": 96 * P * ds + 48 * P + scene_bytes,
+        # camera pass: the hit point (96 B) and the NEE stash (32 B) per pixel; per deferred
+        # specular sample its ray, weight, origin and pixel (52 B)
+        "trace": 96 * P + 32 * P + 52 * S + scene_bytes,
+        # NEE samples written (32 B), read and replaced by the shadow pass (32 + 16 B), summed (16 B);
+        # specular samples read (52 B), replaced (16 B) and summed (16 B)
+        "shadow": 96 * P * ds + 48 * P + 84 * S + scene_bytes,
         "emit": 24 * Ns + scene_bytes,
         "emit_scan": 8 * Ne + 48 * Ns,
         "hash": 16 * Ns + 4 * Ns + 4 * C + 8 * Ns,
@@ -279,7 +284,7 @@ def run_ours(a, cfg: dict) -> dict | None:
     dom = max(kern, key=kern.get)
     per_stage = {}
     for k in ALGO_STAGES:
-        b = algorithmic_bytes(k, Pn, args.photons_per_round, n_s, C, scene_bytes)
+        b = algorithmic_bytes(k, Pn, args.photons_per_round, n_s, C, scene_bytes, S=info.spec_samples)
         t = stages[k]
         per_stage[k] = {"ms": round(t, 4), "algo_bytes": b,
                         "gbs": round(b / (t * 1e-3) / 1e9, 1) if t > 0 else None}

@@ -184,7 +184,8 @@ typedef struct phx_info {
     uint32_t sort_passes;         /* counting-sort digit passes per round */
     uint32_t trav_depth;          /* depth of the device traversal tree */
     uint32_t trav_inner_nodes;    /* inner (child-pair) nodes of the device traversal tree */
-    uint32_t reserved[4];
+    uint32_t spec_samples;        /* specular-NEE shadow rays the last camera pass deferred (all scenes) */
+    uint32_t reserved[3];
 } phx_info;
 
 /* Buffers readable / writable through phx_read_buffer / phx_write_buffer, always in the

@@ -119,7 +119,7 @@ class Info(C.Structure):
                [("total_photons_emitted", C.c_uint64), ("stack_overflows", C.c_uint32), ("error_flags", C.c_uint32),
                 ("_pad0", C.c_uint32 * 2), ("hash", PhotonHashData), ("kernels_per_round", C.c_uint32),
                 ("sort_passes", C.c_uint32), ("trav_depth", C.c_uint32), ("trav_inner_nodes", C.c_uint32),
-                ("reserved", C.c_uint32 * 4)]
+                ("spec_samples", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 class SceneSpec(C.Structure):

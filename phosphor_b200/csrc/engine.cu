@@ -1181,11 +1181,14 @@ int Engine::info(uint32_t s, phx_info *o) {
     o->kernels_per_round = 9 + 3 * o->sort_passes + (tune.nee_wavefront ? 3 : 0) + (spec_deferred() ? 2 : 0) +
                            (tune.gather_sorted && pix_key_bits ? 1 + 3 * radix_passes(pix_key_bits) : 0);
     CK(cudaStreamSynchronize(st));
-    uint32_t v[2] = {0, 0};
+    uint32_t v[3] = {0, 0, 0};
     CK(cudaMemcpy(&v[0], d_ovf.p, 4, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(&v[1], d_err.p, 4, cudaMemcpyDeviceToHost));
+    if (spec_next.p)
+        CK(cudaMemcpy(&v[2], spec_next.p, 4, cudaMemcpyDeviceToHost));
     o->stack_overflows = v[0];
     o->error_flags = v[1];
+    o->spec_samples = spec_deferred() ? std::min(v[2], total_nee) : 0u; // claimed slots, capped as traced
     return PHX_OK;
 }
 
