@@ -486,8 +486,6 @@ void Engine::enq_trace() {
     ev(ST_TRACE, true);
     ev(ST_SHADOW, false);
     launch_shadow(l, o, (int)tune.trace_block, st);
-    if (spec)
-        launch_spec_shadow(l, o, (int)tune.trace_blocks_per_sm, st);
     launch_nee_resolve(l, o, st);
     if (spec)
         launch_spec_resolve(l, o, st);
@@ -1177,8 +1175,8 @@ int Engine::info(uint32_t s, phx_info *o) {
     o->trav_inner_nodes = S.trav_inner;
     // seeds, trace, [shadow, resolve], emit, count scan, compaction, hash, cell scan, 3 per sort
     // pass, records, gather
-    // (+2 with the specular NEE deferred: its shadow kernel and its resolve)
-    o->kernels_per_round = 9 + 3 * o->sort_passes + (tune.nee_wavefront ? 3 : 0) + (spec_deferred() ? 2 : 0) +
+    // (+1 with the specular NEE deferred: its resolve; k_shadow traces its rays)
+    o->kernels_per_round = 9 + 3 * o->sort_passes + (tune.nee_wavefront ? 3 : 0) + (spec_deferred() ? 1 : 0) +
                            (tune.gather_sorted && pix_key_bits ? 1 + 3 * radix_passes(pix_key_bits) : 0);
     CK(cudaStreamSynchronize(st));
     uint32_t v[3] = {0, 0, 0};

@@ -556,7 +556,16 @@ __global__ void __launch_bounds__(128, PHX_TRACE_MINB) k_trace_persistent(Launch
 // ---- shadow wavefront ---------------------------------------------------------------------------
 // One thread per recorded NEE sample; the ds samples of a pixel are consecutive threads, so a warp
 // traces shadow rays from one or two hit points toward the same light: coherent traversal.
-__global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow(LaunchCtx lc, TraceOut out) {
+PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 first_block);
+
+// Blocks [0, nee_blocks): one diffuse sample slot per thread.  Blocks from nee_blocks on (only when
+// the specular NEE is deferred): the specular sample slots, grid-stride; being last in the grid
+// they start as the diffuse blocks drain and fill the launch's tail.
+__global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow(LaunchCtx lc, TraceOut out, u32 nee_blocks) {
+    if (blockIdx.x >= nee_blocks) {
+        shadow_spec_slots(lc, out, nee_blocks);
+        return;
+    }
     const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= lc.total_nee)
         return;
@@ -586,10 +595,11 @@ __global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow(LaunchCtx lc, T
 // Deferred specular NEE samples: one thread per claimed sample slot.  An event's samples are
 // consecutive, so a warp traces rays from one or two hit points toward the lights together.  The
 // contribution is the traced form's: weight * transmittance, zero for a sample without a ray.
-__global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow_spec(LaunchCtx lc, TraceOut out) {
+PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 first_block) {
     const u32 n = min(*out.spec_next, out.spec_cap);
+    const u32 stride = (gridDim.x - first_block) * blockDim.x;
     u32 ovf = 0;
-    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
+    for (u32 g = (blockIdx.x - first_block) * blockDim.x + threadIdx.x; g < n; g += stride) {
         const float4 ray = out.spec_ray[g];
         if (ray.w < 0.0f) {
             out.spec_val[g] = zero4();
@@ -603,6 +613,8 @@ __global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow_spec(LaunchCtx 
     if (ovf)
         atomicAdd(lc.overflow, ovf);
 }
+
+
 
 // Completes the emission of every pixel that deferred a specular NEE term: its listed terms are
 // added to the prefix in path order, an NEE term as throughput * (sum of its samples in sample
@@ -640,12 +652,6 @@ __global__ void __launch_bounds__(256) k_spec_resolve(LaunchCtx lc, TraceOut out
     out.emission[gpix] = (c & DEF_DIFFUSE) ? f4(e.x, e.y, e.z, 1.0f) : e;
 }
 
-void launch_spec_shadow(const LaunchCtx &lc, const TraceOut &out, int blocks_per_sm, cudaStream_t st) {
-    if (!out.spec_ray || out.spec_cap == 0)
-        return;
-    const int grid = g_sm_count * (blocks_per_sm > 0 ? blocks_per_sm : 8);
-    k_shadow_spec<<<grid, 128, 0, st>>>(lc, out);
-}
 
 void launch_spec_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st) {
     if (!out.def_cnt || lc.pix_hi <= lc.pix_lo)
@@ -698,7 +704,9 @@ void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int block, cudaStre
         return;
     if (lc.pix_hi > lc.pix_lo)
         k_nee_sample<<<(lc.pix_hi - lc.pix_lo + 127) / 128, 128, 0, st>>>(lc, out);
-    k_shadow<<<(lc.total_nee + 127) / 128, 128, 0, st>>>(lc, out);
+    const u32 nee_blocks = (lc.total_nee + 127) / 128;
+    const u32 spec_blocks = out.spec_ray && out.spec_cap ? (u32)g_sm_count * 8u : 0u;
+    k_shadow<<<nee_blocks + spec_blocks, 128, 0, st>>>(lc, out, nee_blocks);
 }
 
 void launch_nee_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st) {

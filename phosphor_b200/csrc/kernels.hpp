@@ -61,8 +61,8 @@ void launch_trace(const LaunchCtx &lc, const TraceOut &out, int block, int persi
 // each pixel's samples in sample order into hp_direct.
 void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int block, cudaStream_t st);
 void launch_nee_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st);
-// Deferred specular NEE: trace the claimed sample slots, then complete each listed pixel's emission.
-void launch_spec_shadow(const LaunchCtx &lc, const TraceOut &out, int blocks_per_sm, cudaStream_t st);
+// Deferred specular NEE: complete each listed pixel's emission once k_shadow has traced the
+// claimed sample slots.
 void launch_spec_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st);
 
 struct EmitOut {
