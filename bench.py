@@ -233,12 +233,14 @@ def run_ours(a, cfg: dict) -> dict | None:
     scene = P.SceneData.generate(cfg["kind"], seed=1, width=args.width, height=args.height, detail=cfg["detail"])
     r = P.Renderer(args, device=local)
     r.set_scene(scene)
-    if a.simple or a.persistent or a.concurrent_passes:
+    if a.simple or a.persistent or a.concurrent_passes or a.pipeline_rounds is not None:
         t = r.tuning()
         if a.simple or a.persistent:
             t.persistent = 1 if a.persistent else 0
         if a.concurrent_passes:
             t.concurrent_passes = 1
+        if a.pipeline_rounds is not None:
+            t.pipeline_rounds = a.pipeline_rounds
         r.set_tuning(t)
     tuned = None
     if a.autotune:
@@ -540,6 +542,8 @@ def main() -> int:
     ap.add_argument("--autotune", action="store_true", help="run the library autotuner before timing")
     ap.add_argument("--shard", action="store_true",
                     help="one image over all GPUs (strong scaling) instead of one replica per GPU")
+    ap.add_argument("--pipeline-rounds", type=int, default=None,
+                    help="rounds each graph replay captures and overlaps (1 = off; default: the library's)")
     ap.add_argument("--concurrent-passes", action="store_true",
                     help="camera and photon passes on two branches of the captured round")
     ap.add_argument("--scale", type=int, default=1,

@@ -320,16 +320,21 @@ typedef struct phx_tuning {
     uint32_t concurrent_passes; /* 1 = in the captured graph the camera pass and the photon pass of a
                                    round run on two branches (they only share the round seed) */
     uint32_t gather_sorted;     /* 1 = the gather visits pixels grouped by photon-grid cell */
-    uint32_t reserved[3];
+    uint32_t pipeline_rounds;   /* k > 1: graph replays capture k rounds at a time, each round's camera
+                                   and photon passes on branches of their own (they depend only on
+                                   the round seed) and the gathers in round order, so rounds overlap;
+                                   k - 1 extra sets of per-round buffers (1..8, 1 = off) */
+    uint32_t reserved[2];
 } phx_tuning;
 PHX_API int phx_get_tuning(void *ctx, phx_tuning *out);
 PHX_API int phx_set_tuning(void *ctx, const phx_tuning *in);
 /* Autotuner (no counterpart in the reference): times graph-replayed rounds of this context or batch
  * under candidate tunings — lane refill on/off, NEE wavefront on/off, persistent grid sizes of the
- * camera and photon kernels, concurrent passes on/off — by coordinate descent, keeps the fastest
- * and writes it to *chosen (may be NULL).  Every candidate gives bit-identical results; the SPPM
- * state, seeds and round counters are restored afterwards.  Each trial renders rounds_per_trial + 1
- * rounds (1..64). */
+ * camera and photon kernels, concurrent passes on/off, 1/2/4 rounds in flight — by coordinate
+ * descent, keeps the fastest and writes it to *chosen (may be NULL).  Every candidate gives
+ * bit-identical results; the SPPM state, seeds and round counters are restored afterwards.  Each
+ * trial renders a warm-up group and rounds_per_trial rounds rounded up to whole groups
+ * (rounds_per_trial 1..64); a rounds-in-flight candidate whose buffers do not fit is skipped. */
 PHX_API int phx_autotune(void *ctx, uint32_t rounds_per_trial, phx_tuning *chosen);
 
 /* ---- measurement ------------------------------------------------------------------------------ */

@@ -319,6 +319,8 @@ PHX_API int phx_set_tuning(void *ctx, const phx_tuning *in) {
                 return fail(PHX_E_INVALID, "block sizes must be multiples of 32 up to 1024");
         if (in->trace_blocks_per_sm > 64 || in->emit_blocks_per_sm > 64)
             return fail(PHX_E_INVALID, "blocks_per_sm out of range");
+        if (in->pipeline_rounds > 8)
+            return fail(PHX_E_INVALID, "pipeline_rounds must be at most 8");
         Engine *e = eng(ctx);
         e->tune = *in;
         e->invalidate_graph(); // the next replay is captured with the new launch shape

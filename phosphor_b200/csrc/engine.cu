@@ -48,6 +48,15 @@ Engine::~Engine() {
         cudaStreamSynchronize(st);
     shard_release();
     invalidate_graph();
+    for (auto &v : xbufs)
+        for (auto &b : v)
+            b.release();
+    for (auto s : pipe_st)
+        if (s)
+            cudaStreamDestroy(s);
+    for (auto e : pipe_ev)
+        if (e)
+            cudaEventDestroy(e);
     for (auto &e : events)
         if (e)
             cudaEventDestroy(e);
@@ -383,6 +392,7 @@ int Engine::create(const phx_scene *scenes, const phx_params *params, uint32_t n
         (r = radix_scr.alloc(radix_scratch_bytes(N, key_bits))))
         return r;
     perm = sv0.as<u32>();
+    rs0 = view_own_buffers();
     // gather order: sort the pixels by (cell, octant) key; needs the composite key to fit 32 bits
     pix_key_bits = key_bits + 3 <= 32 ? key_bits + 3 : 0;
     if (pix_key_bits) {
@@ -403,6 +413,7 @@ int Engine::create(const phx_scene *scenes, const phx_params *params, uint32_t n
     tune.nee_wavefront = 1;
     tune.concurrent_passes = 0;
     tune.gather_sorted = 1;
+    tune.pipeline_rounds = 2; // two rounds in flight per graph replay (measured faster, bit-identical)
     for (uint32_t i = 0; i < n; i++)
         if (params[i].flags & PHX_F_SIMPLE_TRAVERSAL)
             tune.persistent = 0;
@@ -410,7 +421,7 @@ int Engine::create(const phx_scene *scenes, const phx_params *params, uint32_t n
     return PHX_OK;
 }
 
-LaunchCtx Engine::lc() const {
+LaunchCtx Engine::lc(const RoundSet &R) const {
     LaunchCtx l;
     l.scenes = d_desc.as<SceneDesc>();
     l.n_scenes = (u32)sc.size();
@@ -418,7 +429,7 @@ LaunchCtx Engine::lc() const {
     l.emit_bases = d_emit_bases.as<u32>();
     l.total_pixels = total_pixels;
     l.total_emit = total_emit;
-    l.seeds = d_seeds.as<u32>();
+    l.seeds = R.seeds;
     l.err = d_err.as<u32>();
     l.overflow = d_ovf.as<u32>();
     l.nee_bases = d_nee_bases.as<u32>();
@@ -431,17 +442,58 @@ LaunchCtx Engine::lc() const {
     return l;
 }
 
-GridBufs Engine::gb() const {
+GridBufs Engine::gb(const RoundSet &R) const {
     GridBufs g;
-    g.counts = counts.as<u32>();
-    g.offsets = offsets.as<u32>();
-    g.slot_pos = slot_pos.as<float4>();
-    g.slot_pd = slot_pd.as<uint2>();
-    g.ph_pos = ph_pos.as<float4>();
-    g.ph_pd = ph_pd.as<uint2>();
-    g.keys = keys.as<u32>();
-    g.cell_count = cell_count.as<u32>();
+    g.counts = R.counts;
+    g.offsets = R.offsets;
+    g.slot_pos = R.slot_pos;
+    g.slot_pd = R.slot_pd;
+    g.ph_pos = R.ph_pos;
+    g.ph_pd = R.ph_pd;
+    g.keys = R.keys;
+    g.cell_count = R.cell_count;
     return g;
+}
+
+RoundSet Engine::view_own_buffers() {
+    RoundSet R;
+    R.seeds = d_seeds.as<u32>();
+    R.queue = d_queue.as<u32>();
+    R.ntotal = d_ntotal.as<u32>();
+    for (int k = 0; k < 6; k++)
+        R.hp[k] = hp[k].as<float4>();
+    R.nee_ray = nee_ray.as<float4>();
+    R.nee_val = nee_val.as<float4>();
+    R.spec_ray = spec_ray.as<float4>();
+    R.spec_val = spec_val.as<float4>();
+    R.spec_org = spec_org.as<float4>();
+    R.spec_pix = spec_pix.as<u32>();
+    R.spec_next = spec_next.as<u32>();
+    R.def_cnt = def_cnt.as<u32>();
+    R.def_prefix = def_prefix.as<float4>();
+    R.def_val = def_val.as<float4>();
+    R.def_tag = def_tag.as<u32>();
+    R.slot_pos = slot_pos.as<float4>();
+    R.slot_pd = slot_pd.as<uint2>();
+    R.counts = counts.as<u32>();
+    R.offsets = offsets.as<u32>();
+    R.ph_pos = ph_pos.as<float4>();
+    R.ph_pd = ph_pd.as<uint2>();
+    R.keys = keys.as<u32>();
+    R.cell_count = cell_count.as<u32>();
+    R.cell_start = cell_start.as<u32>();
+    R.sk0 = sk0.as<u32>();
+    R.sk1 = sk1.as<u32>();
+    R.sv0 = sv0.as<u32>();
+    R.sv1 = sv1.as<u32>();
+    R.s_posdir = s_posdir.as<float4>();
+    R.s_power = s_power.as<u32>();
+    R.s_dir = s_dir.as<float4>();
+    R.s_pow = s_pow.as<float4>();
+    R.scan_scr = scan_scr.p;
+    R.radix_scr = radix_scr.p;
+    R.perm = sv0.as<u32>();
+    return R;
 }
 
 void Engine::ev(int stage, bool end, cudaStream_t s) {
@@ -456,96 +508,87 @@ void Engine::ev(int stage, bool end, cudaStream_t s) {
         cudaEventRecord(e, s ? s : st);
 }
 
-void Engine::enq_seeds() {
-    ev(ST_SEEDS, false);
-    launch_next_seeds(d_rng.as<u32>(), d_seeds.as<u32>(), (u32)sc.size(), st);
-    ev(ST_SEEDS, true);
+void Engine::enq_seeds_r(RoundSet &R, cudaStream_t s) {
+    ev(ST_SEEDS, false, s);
+    launch_next_seeds(d_rng.as<u32>(), R.seeds, (u32)sc.size(), s);
+    ev(ST_SEEDS, true, s);
 }
 
-void Engine::enq_trace() {
-    ev(ST_TRACE, false);
-    TraceOut o{hp[0].as<float4>(), hp[1].as<float4>(), hp[2].as<float4>(), hp[3].as<float4>(),
-               hp[4].as<float4>(), hp[5].as<float4>(), nee_ray.as<float4>(), nee_val.as<float4>()};
-    const LaunchCtx l = lc();
+void Engine::enq_trace_r(RoundSet &R, cudaStream_t s) {
+    ev(ST_TRACE, false, s);
+    TraceOut o{R.hp[0], R.hp[1], R.hp[2], R.hp[3], R.hp[4], R.hp[5], R.nee_ray, R.nee_val};
+    const LaunchCtx l = lc(R);
     const bool spec = spec_deferred();
     if (spec) {
-        o.spec_ray = spec_ray.as<float4>();
-        o.spec_val = spec_val.as<float4>();
-        o.spec_org = spec_org.as<float4>();
-        o.spec_pix = spec_pix.as<u32>();
-        o.spec_next = spec_next.as<u32>();
+        o.spec_ray = R.spec_ray;
+        o.spec_val = R.spec_val;
+        o.spec_org = R.spec_org;
+        o.spec_pix = R.spec_pix;
+        o.spec_next = R.spec_next;
         o.spec_cap = total_nee;
-        o.def_cnt = def_cnt.as<u32>();
-        o.def_prefix = def_prefix.as<float4>();
-        o.def_val = def_val.as<float4>();
-        o.def_tag = def_tag.as<u32>();
-        cudaMemsetAsync(spec_next.p, 0, sizeof(u32), st);
+        o.def_cnt = R.def_cnt;
+        o.def_prefix = R.def_prefix;
+        o.def_val = R.def_val;
+        o.def_tag = R.def_tag;
+        cudaMemsetAsync(R.spec_next, 0, sizeof(u32), s);
     }
-    launch_trace(l, o, (int)tune.trace_block, (int)tune.persistent, (int)tune.trace_blocks_per_sm, d_queue.as<u32>(),
-                 st);
-    ev(ST_TRACE, true);
-    ev(ST_SHADOW, false);
-    launch_shadow(l, o, (int)tune.trace_block, st);
-    launch_nee_resolve(l, o, st);
+    launch_trace(l, o, (int)tune.trace_block, (int)tune.persistent, (int)tune.trace_blocks_per_sm, R.queue, s);
+    ev(ST_TRACE, true, s);
+    ev(ST_SHADOW, false, s);
+    launch_shadow(l, o, (int)tune.trace_block, s);
+    launch_nee_resolve(l, o, s);
     if (spec)
-        launch_spec_resolve(l, o, st);
-    ev(ST_SHADOW, true);
+        launch_spec_resolve(l, o, s);
+    ev(ST_SHADOW, true, s);
     stage_state |= 1;
 }
 
-void Engine::enq_emit(cudaStream_t s) {
-    if (!s)
-        s = st;
+void Engine::enq_emit_r(RoundSet &R, cudaStream_t s) {
     ev(ST_EMIT, false, s);
-    EmitOut o{slot_pos.as<float4>(), slot_pd.as<uint2>(), counts.as<u32>()};
-    launch_emit(lc(), o, (int)tune.emit_block, (int)tune.persistent, (int)tune.emit_blocks_per_sm,
-                d_queue.as<u32>() + 1, s);
+    EmitOut o{R.slot_pos, R.slot_pd, R.counts};
+    launch_emit(lc(R), o, (int)tune.emit_block, (int)tune.persistent, (int)tune.emit_blocks_per_sm, R.queue + 1, s);
     ev(ST_EMIT, true, s);
     ev(ST_EMIT_SCAN, false, s);
-    launch_scan(counts.as<u32>(), offsets.as<u32>(), (u64)total_emit + 1, scan_scr.p, d_ntotal.as<u32>(),
-                d_err.as<u32>(), s);
-    launch_compact(lc(), gb(), s);
+    launch_scan(R.counts, R.offsets, (u64)total_emit + 1, R.scan_scr, R.ntotal, d_err.as<u32>(), s);
+    launch_compact(lc(R), gb(R), s);
     ev(ST_EMIT_SCAN, true, s);
     stage_state |= 2;
 }
 
-void Engine::enq_hash_sort() {
-    ev(ST_HASH, false);
-    cudaMemsetAsync(cell_count.p, 0, 4 * ((size_t)total_cells + 1), st);
-    launch_hash(lc(), gb(), d_ntotal.as<u32>(), max_photons, st);
-    ev(ST_HASH, true);
-    ev(ST_CELL_SCAN, false);
-    launch_scan(cell_count.as<u32>(), cell_start.as<u32>(), (u64)total_cells + 1, scan_scr.p, nullptr,
-                d_err.as<u32>(), st);
-    ev(ST_CELL_SCAN, true);
-    ev(ST_SORT, false);
-    launch_radix_sort(keys.as<u32>(), sk0.as<u32>(), sk1.as<u32>(), sv0.as<u32>(), sv1.as<u32>(), &perm,
-                      d_ntotal.as<u32>(), max_photons, key_bits, radix_scr.p, d_err.as<u32>(), st);
-    ev(ST_SORT, true);
-    ev(ST_RECORDS, false);
-    launch_sorted_records(perm, ph_pos.as<float4>(), ph_pd.as<uint2>(), d_ntotal.as<u32>(), max_photons,
-                          s_posdir.as<float4>(), s_power.as<u32>(), s_dir.as<float4>(), s_pow.as<float4>(),
-                          d_err.as<u32>(), st);
-    ev(ST_RECORDS, true);
+void Engine::enq_hash_sort_r(RoundSet &R, cudaStream_t s) {
+    ev(ST_HASH, false, s);
+    cudaMemsetAsync(R.cell_count, 0, 4 * ((size_t)total_cells + 1), s);
+    launch_hash(lc(R), gb(R), R.ntotal, max_photons, s);
+    ev(ST_HASH, true, s);
+    ev(ST_CELL_SCAN, false, s);
+    launch_scan(R.cell_count, R.cell_start, (u64)total_cells + 1, R.scan_scr, nullptr, d_err.as<u32>(), s);
+    ev(ST_CELL_SCAN, true, s);
+    ev(ST_SORT, false, s);
+    launch_radix_sort(R.keys, R.sk0, R.sk1, R.sv0, R.sv1, &R.perm, R.ntotal, max_photons, key_bits, R.radix_scr,
+                      d_err.as<u32>(), s);
+    ev(ST_SORT, true, s);
+    ev(ST_RECORDS, false, s);
+    launch_sorted_records(R.perm, R.ph_pos, R.ph_pd, R.ntotal, max_photons, R.s_posdir, R.s_power, R.s_dir, R.s_pow,
+                          d_err.as<u32>(), s);
+    ev(ST_RECORDS, true, s);
     stage_state |= 4;
 }
 
-void Engine::enq_gather() {
+void Engine::enq_gather_r(RoundSet &R, cudaStream_t s) {
     adjoint_invalidate();
-    ev(ST_GATHER, false);
+    ev(ST_GATHER, false, s);
     const u32 *order = nullptr;
     if (tune.gather_sorted && pix_key_bits) {
-        launch_pixel_keys(lc(), hp[0].as<float4>(), hp[5].as<float4>(), pk_keys.as<u32>(), st);
+        launch_pixel_keys(lc(R), R.hp[0], R.hp[5], pk_keys.as<u32>(), s);
         launch_radix_sort(pk_keys.as<u32>(), pk_t0.as<u32>(), pk_t1.as<u32>(), pk_v0.as<u32>(), pk_v1.as<u32>(),
-                          &pix_order, d_npix.as<u32>(), total_pixels, pix_key_bits, pk_scr.p, d_err.as<u32>(), st);
+                          &pix_order, d_npix.as<u32>(), total_pixels, pix_key_bits, pk_scr.p, d_err.as<u32>(), s);
         order = pix_order;
     }
-    GatherBufs g{hp[0].as<float4>(), hp[1].as<float4>(), hp[2].as<float4>(), hp[3].as<float4>(),
-                 hp[4].as<float4>(), hp[5].as<float4>(), s_posdir.as<float4>(), s_power.as<u32>(),
-                 s_dir.as<float4>(), s_pow.as<float4>(), cell_start.as<u32>(), (u32)max_photons,
-                 flux.as<float4>(), weight.as<float>(), radiance.as<float4>(), rec_r2, rec_ratio, order};
-    launch_gather(lc(), g, (int)tune.gather_block, st);
-    ev(ST_GATHER, true);
+    GatherBufs g{R.hp[0], R.hp[1], R.hp[2], R.hp[3], R.hp[4], R.hp[5], R.s_posdir, R.s_power, R.s_dir, R.s_pow,
+                 R.cell_start, (u32)max_photons, flux.as<float4>(), weight.as<float>(), radiance.as<float4>(), rec_r2,
+                 rec_ratio, order};
+    launch_gather(lc(R), g, (int)tune.gather_block, s);
+    ev(ST_GATHER, true, s);
 }
 
 void Engine::enq_round() {
@@ -582,10 +625,17 @@ void Engine::invalidate_graph() {
         cudaGraphExecDestroy(gexec_host);
     if (graph_host)
         cudaGraphDestroy(graph_host);
+    if (gexec_pipe)
+        cudaGraphExecDestroy(gexec_pipe);
+    if (graph_pipe)
+        cudaGraphDestroy(graph_pipe);
     gexec = nullptr;
     graph = nullptr;
     gexec_host = nullptr;
     graph_host = nullptr;
+    gexec_pipe = nullptr;
+    graph_pipe = nullptr;
+    pipe_k = 0;
 }
 
 void Engine::set_profiling(bool on) {
@@ -738,6 +788,137 @@ void Engine::count_round(uint32_t rounds) {
     }
 }
 
+// Rounds per pipelined graph: the tuning's, but 1 (off) while profiling stage times, while the
+// adjoint records its forward pass, for a sharded context, or with rounds of the one-thread
+// kernels' inline NEE form (their buffers are the same, this keeps the forms few).
+uint32_t Engine::pipeline_rounds() const {
+    if (tune.pipeline_rounds <= 1 || profiling || rec_r2 || shard.world > 1)
+        return 1;
+    return std::min(tune.pipeline_rounds, 8u);
+}
+
+// Allocates `sets` more sets of per-round buffers, sized like the engine's own (zero-filled where
+// those are).
+int Engine::alloc_round_sets(uint32_t sets) {
+    const size_t P = total_pixels, E = total_emit, C = (size_t)total_cells + 1, N = max_photons,
+                 NE = total_nee, n = sc.size();
+    while (xsets.size() < sets) {
+        std::vector<DevBuf> b(40);
+        RoundSet R;
+        int k = 0, r = 0;
+        auto get = [&](size_t bytes, bool zero) -> void * {
+            DevBuf &d = b[k++];
+            if (r)
+                return nullptr;
+            r = zero ? upload(d, nullptr, bytes) : d.alloc(bytes);
+            return d.p;
+        };
+        R.seeds = (u32 *)get(4 * n, true);
+        R.queue = (u32 *)get(16, true);
+        R.ntotal = (u32 *)get(16, true);
+        for (int h = 0; h < 6; h++)
+            R.hp[h] = (float4 *)get(16 * P, true);
+        R.nee_ray = (float4 *)get(16 * NE, false);
+        R.nee_val = (float4 *)get(16 * NE, false);
+        R.spec_ray = (float4 *)get(16 * NE, false);
+        R.spec_val = (float4 *)get(16 * NE, false);
+        R.spec_org = (float4 *)get(16 * NE, false);
+        R.spec_pix = (u32 *)get(4 * NE, false);
+        R.spec_next = (u32 *)get(16, true);
+        R.def_cnt = (u32 *)get(4 * P, true);
+        R.def_prefix = (float4 *)get(16 * P, false);
+        R.def_val = (float4 *)get(16 * (size_t)DEF_MAX * P, false);
+        R.def_tag = (u32 *)get(4 * (size_t)DEF_MAX * P, false);
+        R.slot_pos = (float4 *)get(16 * N, false);
+        R.slot_pd = (uint2 *)get(8 * N, false);
+        R.counts = (u32 *)get(4 * (E + 1), true);
+        R.offsets = (u32 *)get(4 * (E + 1), true);
+        R.ph_pos = (float4 *)get(16 * N, true);
+        R.ph_pd = (uint2 *)get(8 * N, true);
+        R.keys = (u32 *)get(4 * N, true);
+        R.cell_count = (u32 *)get(4 * C, true);
+        R.cell_start = (u32 *)get(4 * C, true);
+        R.sk0 = (u32 *)get(4 * N, false);
+        R.sk1 = (u32 *)get(4 * N, false);
+        R.sv0 = (u32 *)get(4 * N, true);
+        R.sv1 = (u32 *)get(4 * N, true);
+        R.s_posdir = (float4 *)get(16 * N, true);
+        R.s_power = (u32 *)get(4 * N, true);
+        R.s_dir = (float4 *)get(16 * N, true);
+        R.s_pow = (float4 *)get(16 * N, true);
+        R.scan_scr = get(std::max(scan_scratch_bytes(E + 1), scan_scratch_bytes(C)), false);
+        R.radix_scr = get(radix_scratch_bytes(N, key_bits), false);
+        R.perm = R.sv0;
+        if (r) {
+            for (auto &d : b)
+                d.release();
+            return r;
+        }
+        xbufs.push_back(std::move(b));
+        xsets.push_back(R);
+    }
+    return PHX_OK;
+}
+
+// Captures k rounds.  Round i (0..k-1) uses buffer set k-1-i, so the last round leaves its results
+// in the engine's own buffers (read-back and every other form see the latest round).  The seed
+// steps stay in order on the engine's stream (they advance one RNG state); each round's passes
+// (camera + shadow, photon + hash + sort) run on a branch of their own from its seed step; the
+// gathers run in round order, each after its round's passes.  Rounds thus overlap wherever a
+// round's paths leave the GPU partly idle; every round computes exactly what it computes alone.
+int Engine::capture_pipelined(uint32_t k) {
+    int r;
+    if ((r = alloc_round_sets(k - 1)))
+        return r;
+    while (pipe_st.size() < 2 * k) {
+        cudaStream_t s2;
+        CK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+        pipe_st.push_back(s2);
+    }
+    while (pipe_ev.size() < 3 * k) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        pipe_ev.push_back(e);
+    }
+    auto set = [&](uint32_t i) -> RoundSet & { return i == k - 1 ? rs0 : xsets[k - 2 - i]; };
+    CK(cudaStreamSynchronize(st));
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    capturing = true;
+    for (uint32_t i = 0; i < k; i++) {
+        RoundSet &R = set(i);
+        enq_seeds_r(R, st);
+        cudaEventRecord(pipe_ev[3 * i], st); // round i's seeds
+        cudaStream_t a = pipe_st[2 * i], b = pipe_st[2 * i + 1];
+        cudaStreamWaitEvent(a, pipe_ev[3 * i], 0);
+        if (tune.concurrent_passes) {
+            cudaStreamWaitEvent(b, pipe_ev[3 * i], 0);
+            enq_emit_r(R, b);
+            enq_trace_r(R, a);
+            cudaEventRecord(pipe_ev[3 * i + 1], b);
+            cudaStreamWaitEvent(a, pipe_ev[3 * i + 1], 0);
+        } else {
+            enq_trace_r(R, a);
+            enq_emit_r(R, a);
+        }
+        enq_hash_sort_r(R, a);
+        cudaEventRecord(pipe_ev[3 * i + 2], a); // round i's passes
+    }
+    for (uint32_t i = 0; i < k; i++) {
+        cudaStreamWaitEvent(st, pipe_ev[3 * i + 2], 0);
+        enq_gather_r(set(i), st);
+    }
+    perm = rs0.perm;
+    capturing = false;
+    cudaError_t e = cudaStreamEndCapture(st, &graph_pipe);
+    if (e != cudaSuccess) {
+        graph_pipe = nullptr;
+        return fail(PHX_E_CUDA, std::string("stream capture failed: ") + cudaGetErrorString(e));
+    }
+    CK(cudaGraphInstantiate(&gexec_pipe, graph_pipe, 0));
+    pipe_k = k;
+    return PHX_OK;
+}
+
 int Engine::graph_rounds(uint32_t rounds) {
     if (shard.world > 1)
         return fail(PHX_E_STATE, "a sharded context renders with phx_shard_round or phx_shard_begin/_end");
@@ -745,9 +926,27 @@ int Engine::graph_rounds(uint32_t rounds) {
     if (!any_active())
         return PHX_OK;
     int r;
-    if (!gexec && (r = capture(true, &graph, &gexec)))
+    const uint32_t k = pipeline_rounds();
+    uint32_t single = rounds;
+    if (k > 1 && rounds >= k) {
+        if (pipe_k != k) {
+            if (gexec_pipe)
+                cudaGraphExecDestroy(gexec_pipe);
+            if (graph_pipe)
+                cudaGraphDestroy(graph_pipe);
+            gexec_pipe = nullptr;
+            graph_pipe = nullptr;
+            pipe_k = 0;
+            if ((r = capture_pipelined(k)))
+                return r;
+        }
+        for (uint32_t i = 0; i < rounds / k; i++)
+            CK(cudaGraphLaunch(gexec_pipe, st));
+        single = rounds % k;
+    }
+    if (single && !gexec && (r = capture(true, &graph, &gexec)))
         return r;
-    for (uint32_t i = 0; i < rounds; i++) {
+    for (uint32_t i = 0; i < single; i++) {
         CK(cudaGraphLaunch(gexec, st));
         if (profiling) {
             CK(cudaStreamSynchronize(st));
@@ -834,19 +1033,24 @@ int Engine::autotune(uint32_t rounds, phx_tuning *chosen) {
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
+    // milliseconds per round of `rounds` graph-replayed rounds (rounded up to whole pipelined groups,
+    // after a warm-up that captures the graph)
     auto trial = [&](const phx_tuning &tt, float *ms) -> int {
         tune = tt;
         invalidate_graph();
-        int rr = graph_rounds(1); // capture + warm-up
+        const uint32_t k = pipeline_rounds();
+        const uint32_t n = (rounds + k - 1) / k * k;
+        int rr = graph_rounds(k); // capture + warm-up
         if (rr)
             return rr;
         if (cudaEventRecord(e0, st) != cudaSuccess)
             return fail(PHX_E_CUDA, "event record failed");
-        if ((rr = graph_rounds(rounds)))
+        if ((rr = graph_rounds(n)))
             return rr;
         if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
             cudaEventElapsedTime(ms, e0, e1) != cudaSuccess)
             return fail(PHX_E_CUDA, "event timing failed");
+        *ms /= (float)n;
         return PHX_OK;
     };
     phx_tuning best = tune;
@@ -875,6 +1079,25 @@ int Engine::autotune(uint32_t rounds, phx_tuning *chosen) {
     }
     knob(&phx_tuning::concurrent_passes, {0u, 1u});
     knob(&phx_tuning::gather_sorted, {1u, 0u});
+    // rounds in flight: each more needs another set of per-round buffers; a candidate whose sets do
+    // not fit in device memory is skipped
+    for (uint32_t v : {1u, 2u, 4u}) {
+        if (r || best.pipeline_rounds == v)
+            continue;
+        phx_tuning c = best;
+        c.pipeline_rounds = v;
+        float ms = 0.0f;
+        r = trial(c, &ms);
+        if (r == PHX_E_OOM) {
+            r = PHX_OK;
+            cudaGetLastError();
+            continue;
+        }
+        if (!r && ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     tune = best;

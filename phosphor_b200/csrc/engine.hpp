@@ -64,17 +64,47 @@ struct ShardState {
     uint32_t pix_lo = 0, pix_hi = 0, emit_lo = 0, emit_hi = 0;
 };
 
+// The buffers one round writes and then reads: round seeds, persistent-kernel queues, camera-path
+// outputs and NEE slots, photon slots and canonical photons, cell counts and starts, sort buffers,
+// sorted records, scan and sort scratch.  Set 0 views the engine's own buffers; the pipelined
+// graph form allocates further sets for the earlier rounds of a captured group.  The SPPM state,
+// the error words and the gather's pixel-order buffers stay shared (the gathers run in order).
+struct RoundSet {
+    u32 *seeds = nullptr, *queue = nullptr, *ntotal = nullptr;
+    float4 *hp[6] = {};
+    float4 *nee_ray = nullptr, *nee_val = nullptr;
+    float4 *spec_ray = nullptr, *spec_val = nullptr, *spec_org = nullptr;
+    u32 *spec_pix = nullptr, *spec_next = nullptr, *def_cnt = nullptr;
+    float4 *def_prefix = nullptr, *def_val = nullptr;
+    u32 *def_tag = nullptr;
+    float4 *slot_pos = nullptr;
+    uint2 *slot_pd = nullptr;
+    u32 *counts = nullptr, *offsets = nullptr;
+    float4 *ph_pos = nullptr;
+    uint2 *ph_pd = nullptr;
+    u32 *keys = nullptr, *cell_count = nullptr, *cell_start = nullptr;
+    u32 *sk0 = nullptr, *sk1 = nullptr, *sv0 = nullptr, *sv1 = nullptr;
+    float4 *s_posdir = nullptr;
+    u32 *s_power = nullptr;
+    float4 *s_dir = nullptr, *s_pow = nullptr;
+    void *scan_scr = nullptr, *radix_scr = nullptr;
+    u32 *perm = nullptr; // the photon sort's permutation (set by the hash stage)
+};
+
 class Engine {
   public:
     ~Engine();
     int create(const phx_scene *scenes, const phx_params *params, uint32_t n, int device);
 
-    // enqueue (no host sync)
-    void enq_seeds();
-    void enq_trace();
-    void enq_emit(cudaStream_t s = nullptr); // nullptr: the engine's stream
-    void enq_hash_sort();
-    void enq_gather();
+    // enqueue (no host sync) on the engine's buffers (set 0)
+    void enq_seeds() { enq_seeds_r(rs0, st); }
+    void enq_trace() { enq_trace_r(rs0, st); }
+    void enq_emit(cudaStream_t s = nullptr) { enq_emit_r(rs0, s ? s : st); } // nullptr: the engine's stream
+    void enq_hash_sort() {
+        enq_hash_sort_r(rs0, st);
+        perm = rs0.perm;
+    }
+    void enq_gather() { enq_gather_r(rs0, st); }
     void enq_round();
 
     int plain_round();                // reference form: two host syncs per round
@@ -130,8 +160,29 @@ class Engine {
     int stage_state = 0;
 
   private:
-    LaunchCtx lc() const;
-    GridBufs gb() const;
+    LaunchCtx lc() const { return lc(rs0); }
+    GridBufs gb() const { return gb(rs0); }
+    LaunchCtx lc(const RoundSet &R) const;
+    GridBufs gb(const RoundSet &R) const;
+    void enq_seeds_r(RoundSet &R, cudaStream_t s);
+    void enq_trace_r(RoundSet &R, cudaStream_t s);
+    void enq_emit_r(RoundSet &R, cudaStream_t s);
+    void enq_hash_sort_r(RoundSet &R, cudaStream_t s);
+    void enq_gather_r(RoundSet &R, cudaStream_t s);
+    RoundSet view_own_buffers();
+    RoundSet rs0;
+    // pipelined graph form: `pipe_k` rounds per captured graph, each round's passes on branches of
+    // their own, the gathers in round order; extra buffer sets for all but the last round
+    uint32_t pipeline_rounds() const;
+    int alloc_round_sets(uint32_t sets);
+    int capture_pipelined(uint32_t k);
+    std::vector<std::vector<DevBuf>> xbufs;
+    std::vector<RoundSet> xsets;
+    std::vector<cudaStream_t> pipe_st;
+    std::vector<cudaEvent_t> pipe_ev;
+    cudaGraph_t graph_pipe = nullptr;
+    cudaGraphExec_t gexec_pipe = nullptr;
+    uint32_t pipe_k = 0;
     int upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, uint32_t *pix, uint32_t *emit,
                      uint32_t *cell, uint64_t *slot);
     int scene_photon_range(uint32_t s, uint32_t *off, uint32_t *n);

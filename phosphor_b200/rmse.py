@@ -161,20 +161,27 @@ def time_batched(specs, rounds: int, device: int = 0) -> float:
 
 
 TAIL_CONCURRENT = 2  # active scenes at or below which the camera and photon passes run concurrently
+PIPELINE_ROUNDS = 8  # rounds per captured graph, their passes overlapped (phx_tuning.pipeline_rounds)
 
 
-def time_batched_schedule(specs, r_star: list[int], device: int = 0) -> float:
+def time_batched_schedule(specs, r_star: list[int], device: int = 0, pipeline: int = PIPELINE_ROUNDS) -> float:
     """Wall seconds for the batch in the graph form to give every scene its own number of rounds:
     rounds run for all active scenes, and each scene is retired as soon as it has had r_star[s].
     Once TAIL_CONCURRENT or fewer scenes remain, a round is bound by the latency of their paths and
     the GPU is mostly idle, so the photon pass moves to a concurrent graph branch (measured on the
     16-scene batch: 1.84 -> 1.48 ms per round with one scene left; with all 16 active the branches
-    compete for SM slots and cost time).  Results are bit-identical either way."""
+    compete for SM slots and cost time).  With `pipeline` > 1 each graph replay captures that many
+    rounds and overlaps their camera and photon passes (the gathers stay in order), which shortens
+    the latency-bound rounds of few remaining scenes.  Results are bit-identical either way."""
     b = Batch([s.scene() for s in specs], [s.args() for s in specs], device=device)
     order = sorted(set(r_star))
     done = 0
     active = len(specs)
-    t0 = time.perf_counter()  # includes the graph capture of the first round
+    t0 = time.perf_counter()  # includes the graph capture of the first round and the buffer sets
+    tt = b.tuning()
+    if tt.pipeline_rounds != pipeline:
+        tt.pipeline_rounds = pipeline
+        b.set_tuning(tt)
     for target in order:
         if target > done:
             b.iterate(target - done, graph=True)

@@ -328,6 +328,59 @@ def test_batch_retired_scene_stops_and_others_continue():
     batch.close()
 
 
+PIPE_BUFS = ["FLUX", "PHOTON_WEIGHT", "RADIANCE", "HP_POS", "HP_DIRECT", "HP_EMISSION", "PHOTON_POS",
+             "SORTED_POS", "SORT_PERM", "CELL_START"]
+
+
+@pytest.mark.parametrize("name", ["caustic", "atrium"])
+def test_pipelined_rounds_are_bit_identical(name):
+    """Graph replays that capture k rounds at a time, with each round's passes on branches of their
+    own and the gathers in order, give the bits of rounds replayed one by one: the SPPM state and
+    the last round's hit points, photons and grid (k = 2, 3, 4; 7 rounds, which no k divides)."""
+    scene, args = make(name)
+
+    def run(k):
+        with P.Renderer(args) as r:
+            r.set_scene(scene)
+            t = r.tuning()
+            t.pipeline_rounds = k
+            r.set_tuning(t)
+            r.iterate(3)
+            r.iterate(4)
+            inf = r.info()
+            return {b: r.read(b).view(np.uint32).copy() for b in PIPE_BUFS}, inf.rounds_done, inf.n_photons
+
+    base = run(1)
+    for k in (2, 3, 4):
+        got = run(k)
+        assert got[1:] == base[1:], k
+        for b in PIPE_BUFS:
+            assert np.array_equal(got[0][b], base[0][b]), (k, b)
+
+
+def test_pipelined_batch_with_a_retired_scene():
+    """The pipelined form on a batch, before and after a scene is retired, equals the scenes alone."""
+    specs = [("cornell", dict(photons_per_round=1 << 13, seed=3)),
+             ("caustic", dict(photons_per_round=1 << 12, seed=4)),
+             ("atrium", dict(photons_per_round=1 << 12, seed=5))]
+    made = [make(n, **kw) for n, kw in specs]
+    batch = P.Batch([s for s, _ in made], [a for _, a in made])
+    t = batch.tuning()
+    t.pipeline_rounds, t.concurrent_passes = 2, 1
+    batch.set_tuning(t)
+    batch.iterate(4, graph=True)
+    batch.set_active(1, False)
+    batch.iterate(3, graph=True)
+    assert [batch.info(i).rounds_done for i in range(3)] == [7, 4, 7]
+    for i, (scene, args) in enumerate(made):
+        with P.Renderer(args) as r:
+            r.set_scene(scene)
+            r.iterate(4 if i == 1 else 7)
+            for buf in ["FLUX", "PHOTON_WEIGHT", "RADIANCE"]:
+                assert np.array_equal(batch.read(i, buf).view(np.uint32), r.read(buf).view(np.uint32)), (i, buf)
+    batch.close()
+
+
 def test_autotune_keeps_state_and_results():
     """The autotuner renders trial rounds but restores state, seeds and counters, and the tuning it
     picks gives the same bits as the default one."""
