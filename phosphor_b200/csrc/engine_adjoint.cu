@@ -52,8 +52,9 @@ int Engine::set_materials(const phx_material *m, uint32_t n) {
     S.mats.assign(m, m + n);
     S.desc.any_transmissive = 0;
     for (const auto &mm : S.mats)
-        if (mm.transmission >= 1e-5f)
+        if (!(mm.transmission < 1e-5f)) // not blocking a shadow ray (NaN included)
             S.desc.any_transmissive = 1;
+    invalidate_graph(); // the shadow kernel captured for the scene's kind may no longer fit
     return upload_descs();
 }
 

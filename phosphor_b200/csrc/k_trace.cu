@@ -556,14 +556,16 @@ __global__ void __launch_bounds__(128, PHX_TRACE_MINB) k_trace_persistent(Launch
 // ---- shadow wavefront ---------------------------------------------------------------------------
 // One thread per recorded NEE sample; the ds samples of a pixel are consecutive threads, so a warp
 // traces shadow rays from one or two hit points toward the same light: coherent traversal.
-PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 first_block);
+template <int KIND> PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 first_block);
 
 // Blocks [0, nee_blocks): one diffuse sample slot per thread.  Blocks from nee_blocks on (only when
 // the specular NEE is deferred): the specular sample slots, grid-stride; being last in the grid
-// they start as the diffuse blocks drain and fill the launch's tail.
+// they start as the diffuse blocks drain and fill the launch's tail.  KIND: the scenes' kind
+// (SHADOW_*), chosen on the host.
+template <int KIND>
 __global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow(LaunchCtx lc, TraceOut out, u32 nee_blocks) {
     if (blockIdx.x >= nee_blocks) {
-        shadow_spec_slots(lc, out, nee_blocks);
+        shadow_spec_slots<KIND>(lc, out, nee_blocks);
         return;
     }
     const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -584,7 +586,7 @@ __global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow(LaunchCtx lc, T
     } else {
         u32 ovf = 0;
         const float4 pos = out.pos[gpix];
-        const float4 trans = shadow_transmittance(sc, pos, f4(ray.x, ray.y, ray.z, 0.0f), ray.w, &ovf);
+        const float4 trans = shadow_transmittance<KIND>(sc, pos, f4(ray.x, ray.y, ray.z, 0.0f), ray.w, &ovf);
         contrib = out.nee_val[g] * trans; // frag.radiance * (base / PI) * trans
         if (ovf)
             atomicAdd(lc.overflow, ovf);
@@ -595,7 +597,7 @@ __global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow(LaunchCtx lc, T
 // Deferred specular NEE samples: one thread per claimed sample slot.  An event's samples are
 // consecutive, so a warp traces rays from one or two hit points toward the lights together.  The
 // contribution is the traced form's: weight * transmittance, zero for a sample without a ray.
-PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 first_block) {
+template <int KIND> PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 first_block) {
     const u32 n = min(*out.spec_next, out.spec_cap);
     const u32 stride = (gridDim.x - first_block) * blockDim.x;
     u32 ovf = 0;
@@ -607,7 +609,8 @@ PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 firs
         }
         const u32 gpix = out.spec_pix[g];
         const SceneDesc &sc = lc.scenes[lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gpix)];
-        const float4 trans = shadow_transmittance(sc, out.spec_org[g], f4(ray.x, ray.y, ray.z, 0.0f), ray.w, &ovf);
+        const float4 trans =
+            shadow_transmittance<KIND>(sc, out.spec_org[g], f4(ray.x, ray.y, ray.z, 0.0f), ray.w, &ovf);
         out.spec_val[g] = out.spec_val[g] * trans;
     }
     if (ovf)
@@ -698,15 +701,17 @@ __global__ void __launch_bounds__(128) k_nee_sample(LaunchCtx lc, TraceOut out) 
     record_nee(sc, &rng, out.pos[gpix], sn, out.base_color[gpix], out, slot);
 }
 
-void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int block, cudaStream_t st) {
-    (void)block;
+void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int kind, cudaStream_t st) {
     if (!lc.nee_defer || lc.total_nee == 0)
         return;
     if (lc.pix_hi > lc.pix_lo)
         k_nee_sample<<<(lc.pix_hi - lc.pix_lo + 127) / 128, 128, 0, st>>>(lc, out);
     const u32 nee_blocks = (lc.total_nee + 127) / 128;
     const u32 spec_blocks = out.spec_ray && out.spec_cap ? (u32)g_sm_count * 8u : 0u;
-    k_shadow<<<nee_blocks + spec_blocks, 128, 0, st>>>(lc, out, nee_blocks);
+    if (kind == SHADOW_OPAQUE)
+        k_shadow<SHADOW_OPAQUE><<<nee_blocks + spec_blocks, 128, 0, st>>>(lc, out, nee_blocks);
+    else
+        k_shadow<SHADOW_GENERAL><<<nee_blocks + spec_blocks, 128, 0, st>>>(lc, out, nee_blocks);
 }
 
 void launch_nee_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st) {

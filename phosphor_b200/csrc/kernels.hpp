@@ -59,7 +59,8 @@ void launch_trace(const LaunchCtx &lc, const TraceOut &out, int block, int persi
                   u32 *queue, cudaStream_t st);
 // Deferred diffuse-hit NEE: trace every recorded shadow ray (one thread per sample slot), then sum
 // each pixel's samples in sample order into hp_direct.
-void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int block, cudaStream_t st);
+// kind: SHADOW_OPAQUE when no scene has a transmissive material, else SHADOW_GENERAL.
+void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int kind, cudaStream_t st);
 void launch_nee_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st);
 // Deferred specular NEE: complete each listed pixel's emission once k_shadow has traced the
 // claimed sample slots.
