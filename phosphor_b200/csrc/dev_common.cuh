@@ -127,6 +127,24 @@ PHX_HDI u32 random_u32(Rng *rng) {
 }
 PHX_HDI float random_float(Rng *rng) { return (float)random_u32(rng) / U32_MAX_F; }
 
+// The state after n more draws, in O(log n) steps: the LCG's n-step map x -> A x + C, composed by
+// binary powering (Brown, "Random number generation with arbitrary strides", Trans. Am. Nucl. Soc.
+// 71, 1994).  All arithmetic is mod 2^32, so the result equals n calls of random_u32 exactly.
+PHX_HDI Rng rng_advance(Rng r, u32 n) {
+    u32 cur_mult = 747796405u, cur_plus = 2891336453u, acc_mult = 1u, acc_plus = 0u;
+    while (n) {
+        if (n & 1u) {
+            acc_mult *= cur_mult;
+            acc_plus = acc_plus * cur_mult + cur_plus;
+        }
+        cur_plus = (cur_mult + 1u) * cur_plus;
+        cur_mult *= cur_mult;
+        n >>= 1;
+    }
+    r.state = acc_mult * r.state + acc_plus;
+    return r;
+}
+
 // utils.h:59-71
 PHX_HDI void make_tbn(float4 normal, float4 *tangent, float4 *bitangent) {
     normal.w = 0.0f;

@@ -70,7 +70,9 @@ struct __align__(16) SceneDesc {
     u32 any_transmissive; // 0 -> shadow rays can stop at the first hit
     u32 nee_base;         // first deferred-NEE sample slot of this scene (pixel i, sample d at nee_base + i*ds + d)
     u32 active;           // 0: a batch scene that has been retired; every stage skips it
+    u32 light_draws;      // RNG draws of one light sample when the same for every light, else LIGHT_DRAWS_VARY
 };
+constexpr u32 LIGHT_DRAWS_VARY = 0xffffffffu;
 
 // scene of global index gid: bases[s] <= gid < bases[s+1] (n+1 prefix offsets)
 PHX_DI u32 find_scene(const u32 *bases, u32 n, u32 gid) {

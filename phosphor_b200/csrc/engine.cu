@@ -68,7 +68,8 @@ Engine::~Engine() {
     for (auto &s : sc)
         for (auto &b : s.bufs)
             b.release();
-    DevBuf *all[] = {&d_desc, &d_pix_bases, &d_emit_bases, &d_nee_bases, &nee_ray, &nee_val, &spec_ray, &spec_val,
+    DevBuf *all[] = {&d_desc, &d_pix_bases, &d_emit_bases, &d_nee_bases, &nee_ray, &nee_val, &stash_sn, &stash_rng,
+                     &spec_ray, &spec_val,
                      &spec_org, &spec_pix, &spec_next, &def_cnt, &def_prefix, &def_val, &def_tag, &d_seeds, &d_rng,
                      &d_err, &d_ovf, &d_queue, &d_ntotal,
                      &flux, &weight, &radiance, &slot_pos, &slot_pd, &counts, &offsets, &ph_pos, &ph_pd, &keys,
@@ -116,6 +117,32 @@ static int check_params(const phx_params &p) {
     if (!(p.sppm_alpha >= 0.0f))
         return fail(PHX_E_INVALID, "sppm_alpha must be non-negative");
     return PHX_OK;
+}
+
+// RNG draws one light sample takes (sample_light_fragment): none without light, one to choose the
+// light, and for an area light of nonzero area one more to choose its triangle (when it has
+// several) and two for the point.  LIGHT_DRAWS_VARY when the lights differ: a sample's draws then
+// depend on which light it chose.
+uint32_t light_sample_draws(const phx_light *l, uint32_t n, float total_lum) {
+    const float eps = 1e-5f;
+    if (n == 0 || total_lum < eps)
+        return 0;
+    uint32_t draws = LIGHT_DRAWS_VARY;
+    for (uint32_t k = 0; k < n; k++) {
+        uint32_t d = 1;
+        if (l[k].kind != PHX_LIGHT_POINT && l[k].kind != PHX_LIGHT_SPOT && l[k].kind != PHX_LIGHT_DIRECTIONAL) {
+            const float area = l[k].aux.w;
+            uint32_t ntri;
+            std::memcpy(&ntri, &l[k].aux.z, 4);
+            if (!(area < eps))
+                d = 1 + ((ntri <= 1 || area <= eps) ? 0 : 1) + 2;
+        }
+        if (k == 0)
+            draws = d;
+        else if (d != draws)
+            return LIGHT_DRAWS_VARY;
+    }
+    return draws;
 }
 
 int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, uint32_t *pix, uint32_t *emit,
@@ -270,6 +297,7 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
     d.n_tris = n;
     d.n_lights = s.n_lights;
     d.total_lum = s.n_lights ? lum[s.n_lights - 1] : 0.0f; // shading.cpp:26
+    d.light_draws = light_sample_draws(s.lights, s.n_lights, d.total_lum);
     phx_f4 ctr;
     float rad;
     scene_sphere(S.nodes[0], &ctr, &rad);
@@ -365,6 +393,7 @@ int Engine::create(const phx_scene *scenes, const phx_params *params, uint32_t n
     if ((r = upload(d_desc, descs.data(), sizeof(SceneDesc) * n)) || (r = upload(d_pix_bases, pb.data(), 4 * pb.size())) ||
         (r = upload(d_emit_bases, eb.data(), 4 * eb.size())) || (r = upload(d_nee_bases, nb.data(), 4 * nb.size())) ||
         (r = nee_ray.alloc(16 * (size_t)total_nee)) || (r = nee_val.alloc(16 * (size_t)total_nee)) ||
+        (r = stash_sn.alloc(16 * (size_t)total_pixels)) || (r = stash_rng.alloc(4 * (size_t)total_pixels)) ||
         (r = spec_ray.alloc(16 * (size_t)total_nee)) || (r = spec_val.alloc(16 * (size_t)total_nee)) ||
         (r = spec_org.alloc(16 * (size_t)total_nee)) || (r = spec_pix.alloc(4 * (size_t)total_nee)) ||
         (r = upload(spec_next, nullptr, 16)) || (r = upload(def_cnt, nullptr, 4 * (size_t)total_pixels)) ||
@@ -464,6 +493,8 @@ RoundSet Engine::view_own_buffers() {
         R.hp[k] = hp[k].as<float4>();
     R.nee_ray = nee_ray.as<float4>();
     R.nee_val = nee_val.as<float4>();
+    R.stash_sn = stash_sn.as<float4>();
+    R.stash_rng = stash_rng.as<u32>();
     R.spec_ray = spec_ray.as<float4>();
     R.spec_val = spec_val.as<float4>();
     R.spec_org = spec_org.as<float4>();
@@ -516,7 +547,7 @@ void Engine::enq_seeds_r(RoundSet &R, cudaStream_t s) {
 
 void Engine::enq_trace_r(RoundSet &R, cudaStream_t s) {
     ev(ST_TRACE, false, s);
-    TraceOut o{R.hp[0], R.hp[1], R.hp[2], R.hp[3], R.hp[4], R.hp[5], R.nee_ray, R.nee_val};
+    TraceOut o{R.hp[0], R.hp[1], R.hp[2], R.hp[3], R.hp[4], R.hp[5], R.nee_ray, R.nee_val, R.stash_sn, R.stash_rng};
     const LaunchCtx l = lc(R);
     const bool spec = spec_deferred();
     if (spec) {
@@ -535,10 +566,12 @@ void Engine::enq_trace_r(RoundSet &R, cudaStream_t s) {
     launch_trace(l, o, (int)tune.trace_block, (int)tune.persistent, (int)tune.trace_blocks_per_sm, R.queue, s);
     ev(ST_TRACE, true, s);
     ev(ST_SHADOW, false, s);
-    bool transmissive = false;
-    for (const auto &sl : sc)
+    bool transmissive = false, presample = false;
+    for (const auto &sl : sc) {
         transmissive = transmissive || sl.desc.any_transmissive != 0;
-    launch_shadow(l, o, transmissive ? SHADOW_GENERAL : SHADOW_OPAQUE, s);
+        presample = presample || sl.desc.light_draws == LIGHT_DRAWS_VARY;
+    }
+    launch_shadow(l, o, transmissive ? SHADOW_GENERAL : SHADOW_OPAQUE, presample, s);
     launch_nee_resolve(l, o, s);
     if (spec)
         launch_spec_resolve(l, o, s);
@@ -806,7 +839,7 @@ int Engine::alloc_round_sets(uint32_t sets) {
     const size_t P = total_pixels, E = total_emit, C = (size_t)total_cells + 1, N = max_photons,
                  NE = total_nee, n = sc.size();
     while (xsets.size() < sets) {
-        std::vector<DevBuf> b(40);
+        std::vector<DevBuf> b(44);
         RoundSet R;
         int k = 0, r = 0;
         auto get = [&](size_t bytes, bool zero) -> void * {
@@ -823,6 +856,8 @@ int Engine::alloc_round_sets(uint32_t sets) {
             R.hp[h] = (float4 *)get(16 * P, true);
         R.nee_ray = (float4 *)get(16 * NE, false);
         R.nee_val = (float4 *)get(16 * NE, false);
+        R.stash_sn = (float4 *)get(16 * P, false);
+        R.stash_rng = (u32 *)get(4 * P, false);
         R.spec_ray = (float4 *)get(16 * NE, false);
         R.spec_val = (float4 *)get(16 * NE, false);
         R.spec_org = (float4 *)get(16 * NE, false);
@@ -1399,10 +1434,14 @@ int Engine::info(uint32_t s, phx_info *o) {
     o->sort_passes = radix_passes(key_bits);
     o->trav_depth = S.trav_depth;
     o->trav_inner_nodes = S.trav_inner;
-    // seeds, trace, [shadow, resolve], emit, count scan, compaction, hash, cell scan, 3 per sort
-    // pass, records, gather
-    // (+1 with the specular NEE deferred: its resolve; k_shadow traces its rays)
-    o->kernels_per_round = 9 + 3 * o->sort_passes + (tune.nee_wavefront ? 3 : 0) + (spec_deferred() ? 1 : 0) +
+    // seeds, trace, [sample, shadow, resolve], emit, count scan, compaction, hash, cell scan, 3 per
+    // sort pass, records, gather (+1 with the specular NEE deferred: its resolve; k_shadow traces
+    // its rays).  The sampling kernel runs only for scenes whose light samples vary in RNG draws.
+    bool presample = false;
+    for (const auto &sl : sc)
+        presample = presample || sl.desc.light_draws == LIGHT_DRAWS_VARY;
+    o->kernels_per_round = 9 + 3 * o->sort_passes + (tune.nee_wavefront ? (presample ? 3 : 2) : 0) +
+                           (spec_deferred() ? 1 : 0) +
                            (tune.gather_sorted && pix_key_bits ? 1 + 3 * radix_passes(pix_key_bits) : 0);
     CK(cudaStreamSynchronize(st));
     uint32_t v[3] = {0, 0, 0};

@@ -72,7 +72,8 @@ struct ShardState {
 struct RoundSet {
     u32 *seeds = nullptr, *queue = nullptr, *ntotal = nullptr;
     float4 *hp[6] = {};
-    float4 *nee_ray = nullptr, *nee_val = nullptr;
+    float4 *nee_ray = nullptr, *nee_val = nullptr, *stash_sn = nullptr;
+    u32 *stash_rng = nullptr;
     float4 *spec_ray = nullptr, *spec_val = nullptr, *spec_org = nullptr;
     u32 *spec_pix = nullptr, *spec_next = nullptr, *def_cnt = nullptr;
     float4 *def_prefix = nullptr, *def_val = nullptr;
@@ -90,6 +91,8 @@ struct RoundSet {
     void *scan_scr = nullptr, *radix_scr = nullptr;
     u32 *perm = nullptr; // the photon sort's permutation (set by the hash stage)
 };
+
+uint32_t light_sample_draws(const phx_light *l, uint32_t n, float total_lum);
 
 class Engine {
   public:
@@ -192,7 +195,7 @@ class Engine {
     void accumulate_profile();
 
     DevBuf d_desc, d_pix_bases, d_emit_bases, d_nee_bases, d_seeds, d_rng, d_err, d_ovf, d_queue, d_ntotal;
-    DevBuf nee_ray, nee_val;
+    DevBuf nee_ray, nee_val, stash_sn, stash_rng;
     // deferred specular NEE: sample slots (as many as the diffuse ones) and per-pixel term lists
     DevBuf spec_ray, spec_val, spec_org, spec_pix, spec_next, def_cnt, def_prefix, def_val, def_tag;
     bool spec_deferred() const { return tune.persistent && tune.nee_wavefront && total_nee > 0; }

@@ -78,6 +78,8 @@ int Engine::set_lights(const phx_light *l, uint32_t n) {
     CK(cudaMemcpy(S.bufs[14].p, lum.data(), 4 * (size_t)n, cudaMemcpyHostToDevice));
     S.lights.assign(l, l + n);
     S.desc.total_lum = lum[n - 1]; // shading.cpp:26
+    S.desc.light_draws = light_sample_draws(l, n, S.desc.total_lum);
+    invalidate_graph(); // the captured shadow stage depends on the draw count
     return upload_descs();
 }
 

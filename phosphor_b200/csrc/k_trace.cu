@@ -59,9 +59,9 @@ PHX_DI void write_result(const TraceOut &out, u32 gpix, const TraceResult &r) {
 // The camera kernels only leave the pixel's RNG state and shading normal in its first sample slot
 // (stash_nee): drawing the samples there would run the light-sampling code for one lane of a warp
 // at a time, while k_nee_sample runs it for 32 diffuse hit points together.
-PHX_DI void stash_nee(const TraceOut &out, u32 slot, Rng rng, float4 sn) {
-    out.nee_ray[slot] = sn;
-    out.nee_val[slot] = f4(__uint_as_float(rng.state), 0.0f, 0.0f, 0.0f);
+PHX_DI void stash_nee(const TraceOut &out, u32 gpix, Rng rng, float4 sn) {
+    out.stash_sn[gpix] = sn;
+    out.stash_rng[gpix] = rng.state;
 }
 
 PHX_DI void record_nee(const SceneDesc &sc, Rng *rng, float4 pos, float4 sn, float4 base, const TraceOut &out,
@@ -116,7 +116,7 @@ PHX_DI void trace_pixel(const SceneDesc &sc, u32 seed, u32 tid, const TraceOut &
         BsdfSample bs = sample_bsdf(&rng, ctx, ctx.shading_normal, sh.normal, view, &ior, sh.front_face);
         if (bs.event == BSDF_DIFFUSE) {
             if (defer) {
-                stash_nee(out, sc.nee_base + tid * sc.direct_samples, rng, ctx.shading_normal);
+                stash_nee(out, gpix, rng, ctx.shading_normal);
                 direct = f4(ctx.occlusion, 0.0f, 0.0f, 0.0f); // the resolve kernel completes it
             } else {
                 float4 sum = zero4();
@@ -261,27 +261,38 @@ PHX_DI void cp_start(CameraPath &p, const SceneDesc *sc, u32 seed, u32 tid, u32 
     p.t_max = INF;
 }
 
+// Whether a scene's specular NEE samples are drawn by the shadow kernel (each thread its own
+// sample, from the event's RNG state advanced past the samples before it): possible when every
+// light sample takes the same number of draws; the event record needs four sample slots.
+PHX_DI bool spec_drawn_in_shadow(const SceneDesc &sc) {
+    return sc.light_draws != LIGHT_DRAWS_VARY && sc.direct_samples >= 4;
+}
+
 // One sample of direct_lighting_specular (light_sampling.h:355-390) up to its shadow query: false
 // when it contributes nothing (no RNG draw depends on a shadow query's outcome), else the light
 // fragment and the weight m of its transmittance.
-PHX_DI bool spec_sample(CameraPath &p, LightFragment *f, float4 *m) {
-    const SceneDesc &sc = *p.sc;
-    float ndv = dot(p.view, p.sn);
+PHX_DI bool spec_light_sample(Rng *rng, const SceneDesc &sc, float4 pos, float4 sn, float4 view, float4 f0,
+                              float rough, LightFragment *f, float4 *m) {
+    float ndv = dot(view, sn);
     if (ndv < EPS)
         return false;
-    if (!sample_light_fragment(&p.rng, sc, p.pos, p.sn, f) || f->n_dot_dir < EPS)
+    if (!sample_light_fragment(rng, sc, pos, sn, f) || f->n_dot_dir < EPS)
         return false;
-    float alpha = p.rough * p.rough;
-    float4 h = normalize(f->dir + p.view);
-    float ndh = fmaxf(dot(p.sn, h), 0.0f);
+    float alpha = rough * rough;
+    float4 h = normalize(f->dir + view);
+    float ndh = fmaxf(dot(sn, h), 0.0f);
     float g = ggx_ndf(ndh, alpha);
-    float4 fr = fresnel4(p.f0, p.view, h);
+    float4 fr = fresnel4(f0, view, h);
     float sm = smith_g1_ggx(f->n_dot_dir, alpha) * smith_g1_ggx(ndv, alpha);
     float4 spec = f->radiance * g * fr * sm / (4.0f * f->n_dot_dir * ndv);
     if (dot(spec, spec) < EPS * EPS)
         return false;
     *m = spec;
     return true;
+}
+
+PHX_DI bool spec_sample(CameraPath &p, LightFragment *f, float4 *m) {
+    return spec_light_sample(&p.rng, *p.sc, p.pos, p.sn, p.view, p.f0, p.rough, f, m);
 }
 
 // Runs the NEE loop from sample nee_i until a shadow query is needed (returns true with the query
@@ -380,17 +391,37 @@ static __device__ __noinline__ bool cp_defer_specular(CameraPath &p, const Trace
     const u32 ds = p.sc->direct_samples;
     if (p.def_n >= DEF_MAX)
         return false;
+    const bool drawn_later = spec_drawn_in_shadow(*p.sc);
     const u32 base = claim_slots(out.spec_next, ds);
     if (ds > out.spec_cap || base > out.spec_cap - ds) {
         // no room: the slots of this claim that lie below the capacity carry no ray
         for (u32 slot = base; slot < out.spec_cap && slot - base < ds; slot++) {
-            out.spec_ray[slot] = f4(0.0f, 0.0f, 0.0f, -1.0f);
+            out.spec_ray[slot] = drawn_later ? f4(__uint_as_float(slot), 0.0f, 0.0f, __uint_as_float(1u))
+                                             : f4(0.0f, 0.0f, 0.0f, -1.0f);
             out.spec_val[slot] = zero4();
             out.spec_org[slot] = zero4();
             out.spec_pix[slot] = p.gpix;
         }
         return false;
     }
+    if (drawn_later) {
+        // k_shadow draws sample i from this state advanced by i * light_draws; here the event is
+        // recorded in its first four slots' origins and every slot's header, and the path's RNG
+        // skips the event's draws (none when the view grazes: every sample fails before drawing)
+        const bool grazing = dot(p.view, p.sn) < EPS;
+        out.spec_org[base] = p.pos;
+        out.spec_org[base + 1] = p.sn;
+        out.spec_org[base + 2] = p.view;
+        out.spec_org[base + 3] = p.f0;
+        const float4 hdr = f4(__uint_as_float(base), p.rough, __uint_as_float(p.rng.state),
+                              __uint_as_float(grazing ? 1u : 0u));
+        for (u32 i = 0; i < ds; i++) {
+            out.spec_ray[base + i] = hdr;
+            out.spec_pix[base + i] = p.gpix;
+        }
+        if (!grazing)
+            p.rng = rng_advance(p.rng, ds * p.sc->light_draws);
+    } else {
     for (u32 i = 0; i < ds; i++) {
         LightFragment f;
         float4 m;
@@ -404,6 +435,7 @@ static __device__ __noinline__ bool cp_defer_specular(CameraPath &p, const Trace
         }
         out.spec_org[slot] = p.pos;
         out.spec_pix[slot] = p.gpix;
+    }
     }
     const size_t k = (size_t)p.gpix * DEF_MAX + p.def_n++;
     out.def_val[k] = p.throughput;
@@ -488,7 +520,7 @@ PHX_DI bool cp_advance(CameraPath &p, bool hit, const Hit &h, const TraceOut &ou
     if (bs.event == BSDF_DIFFUSE) {
         p.nee_kind = NEE_DIFFUSE;
         if (defer) {
-            stash_nee(out, sc.nee_base + p.tid * sc.direct_samples, p.rng, p.sn);
+            stash_nee(out, p.gpix, p.rng, p.sn);
             cp_finish(p, out, true, true);
             return false;
         }
@@ -575,19 +607,37 @@ __global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow(LaunchCtx lc, T
     const SceneDesc &sc = lc.scenes[s];
     if (!sc.active)
         return;
-    const u32 pixel = (g - sc.nee_base) / sc.direct_samples;
+    const u32 ds = sc.direct_samples;
+    const u32 pixel = (g - sc.nee_base) / ds;
     const u32 gpix = sc.pixel_base + pixel;
     if (out.emission[gpix].w != 1.0f)
         return; // no diffuse hit point: the slot was not used this round
-    const float4 ray = out.nee_ray[g];
-    float4 contrib;
-    if (ray.w < 0.0f) {
-        contrib = zero4(); // sample_light_fragment failed: direct_lighting_diffuse returned BLACK
-    } else {
+    const float4 pos = out.pos[gpix];
+    float4 dir = zero4(), w = zero4();
+    float dist = -1.0f; // < 0: sample_light_fragment failed, direct_lighting_diffuse returns BLACK
+    if (sc.light_draws != LIGHT_DRAWS_VARY) {
+        // this slot's sample, drawn here: the pixel's stream advanced past the samples before it
+        Rng rng;
+        rng.state = out.stash_rng[gpix];
+        rng = rng_advance(rng, (g - sc.nee_base - pixel * ds) * sc.light_draws);
+        LightFragment f;
+        if (sample_light_fragment(&rng, sc, pos, out.stash_sn[gpix], &f)) { // light_sampling.h:345-352
+            dir = f4(f.dir.x, f.dir.y, f.dir.z, 0.0f);
+            dist = f.dist;
+            w = f.radiance * (out.base_color[gpix] / PI);
+        }
+    } else { // drawn by k_nee_sample
+        const float4 ray = out.nee_ray[g];
+        if (!(ray.w < 0.0f)) {
+            dir = f4(ray.x, ray.y, ray.z, 0.0f);
+            dist = ray.w;
+            w = out.nee_val[g];
+        }
+    }
+    float4 contrib = zero4();
+    if (!(dist < 0.0f)) {
         u32 ovf = 0;
-        const float4 pos = out.pos[gpix];
-        const float4 trans = shadow_transmittance<KIND>(sc, pos, f4(ray.x, ray.y, ray.z, 0.0f), ray.w, &ovf);
-        contrib = out.nee_val[g] * trans; // frag.radiance * (base / PI) * trans
+        contrib = w * shadow_transmittance<KIND>(sc, pos, dir, dist, &ovf); // frag.radiance * (base / PI) * trans
         if (ovf)
             atomicAdd(lc.overflow, ovf);
     }
@@ -602,16 +652,41 @@ template <int KIND> PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const Tra
     const u32 stride = (gridDim.x - first_block) * blockDim.x;
     u32 ovf = 0;
     for (u32 g = (blockIdx.x - first_block) * blockDim.x + threadIdx.x; g < n; g += stride) {
-        const float4 ray = out.spec_ray[g];
-        if (ray.w < 0.0f) {
-            out.spec_val[g] = zero4();
-            continue;
-        }
         const u32 gpix = out.spec_pix[g];
         const SceneDesc &sc = lc.scenes[lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gpix)];
-        const float4 trans =
-            shadow_transmittance<KIND>(sc, out.spec_org[g], f4(ray.x, ray.y, ray.z, 0.0f), ray.w, &ovf);
-        out.spec_val[g] = out.spec_val[g] * trans;
+        const float4 hdr = out.spec_ray[g];
+        float4 org, dir = zero4(), w = zero4();
+        float dist = -1.0f; // < 0: no contribution
+        if (spec_drawn_in_shadow(sc)) {
+            // the event recorded by the camera pass: header (first slot, roughness, RNG state,
+            // grazing view), origin / shading normal / view / f0 in its first four slots
+            const u32 base = __float_as_uint(hdr.x);
+            org = out.spec_org[base];
+            if (__float_as_uint(hdr.w) == 0u) {
+                Rng rng;
+                rng.state = __float_as_uint(hdr.z);
+                rng = rng_advance(rng, (g - base) * sc.light_draws);
+                LightFragment f;
+                float4 m;
+                if (spec_light_sample(&rng, sc, org, out.spec_org[base + 1], out.spec_org[base + 2],
+                                      out.spec_org[base + 3], hdr.y, &f, &m)) {
+                    dir = f4(f.dir.x, f.dir.y, f.dir.z, 0.0f);
+                    dist = f.dist;
+                    w = m;
+                }
+            }
+        } else { // drawn by the camera pass
+            org = out.spec_org[g];
+            if (!(hdr.w < 0.0f)) {
+                dir = f4(hdr.x, hdr.y, hdr.z, 0.0f);
+                dist = hdr.w;
+                w = out.spec_val[g];
+            }
+        }
+        float4 contrib = zero4();
+        if (!(dist < 0.0f))
+            contrib = w * shadow_transmittance<KIND>(sc, org, dir, dist, &ovf);
+        out.spec_val[g] = contrib;
     }
     if (ovf)
         atomicAdd(lc.overflow, ovf);
@@ -692,19 +767,18 @@ __global__ void __launch_bounds__(128) k_nee_sample(LaunchCtx lc, TraceOut out) 
         return; // no diffuse hit point
     const u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gpix);
     const SceneDesc &sc = lc.scenes[s];
-    if (!sc.active)
+    if (!sc.active || sc.light_draws != LIGHT_DRAWS_VARY) // fixed draws: k_shadow draws each sample
         return;
     const u32 slot = sc.nee_base + (gpix - sc.pixel_base) * sc.direct_samples;
-    const float4 sn = out.nee_ray[slot];
     Rng rng;
-    rng.state = __float_as_uint(out.nee_val[slot].x);
-    record_nee(sc, &rng, out.pos[gpix], sn, out.base_color[gpix], out, slot);
+    rng.state = out.stash_rng[gpix];
+    record_nee(sc, &rng, out.pos[gpix], out.stash_sn[gpix], out.base_color[gpix], out, slot);
 }
 
-void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int kind, cudaStream_t st) {
+void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int kind, bool presample, cudaStream_t st) {
     if (!lc.nee_defer || lc.total_nee == 0)
         return;
-    if (lc.pix_hi > lc.pix_lo)
+    if (presample && lc.pix_hi > lc.pix_lo)
         k_nee_sample<<<(lc.pix_hi - lc.pix_lo + 127) / 128, 128, 0, st>>>(lc, out);
     const u32 nee_blocks = (lc.total_nee + 127) / 128;
     const u32 spec_blocks = out.spec_ray && out.spec_cap ? (u32)g_sm_count * 8u : 0u;

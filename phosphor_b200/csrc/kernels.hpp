@@ -39,6 +39,8 @@ struct TraceOut {
     float4 *pos, *normal, *throughput, *base_color, *direct, *emission;
     float4 *nee_ray; // per NEE sample slot: (dir.xyz, light distance), w < 0 = no contribution
     float4 *nee_val; // per slot: radiance * (base / pi); replaced by the contribution in the shadow pass
+    float4 *stash_sn = nullptr; // per pixel with a diffuse hit point: shading normal for its NEE samples
+    u32 *stash_rng = nullptr;   // per pixel: RNG state at its NEE samples
     // Deferred specular NEE (lane-refill camera kernel; null: traced in place).  Each specular
     // event claims direct_samples consecutive sample slots; from a pixel's first deferred event on,
     // its nonzero emission terms are listed in order and summed once the samples are traced.
@@ -59,8 +61,9 @@ void launch_trace(const LaunchCtx &lc, const TraceOut &out, int block, int persi
                   u32 *queue, cudaStream_t st);
 // Deferred diffuse-hit NEE: trace every recorded shadow ray (one thread per sample slot), then sum
 // each pixel's samples in sample order into hp_direct.
-// kind: SHADOW_OPAQUE when no scene has a transmissive material, else SHADOW_GENERAL.
-void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int kind, cudaStream_t st);
+// kind: SHADOW_OPAQUE when no scene has a transmissive material, else SHADOW_GENERAL.  presample:
+// some scene's light samples take varying RNG draws, so k_nee_sample draws its samples first.
+void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int kind, bool presample, cudaStream_t st);
 void launch_nee_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st);
 // Deferred specular NEE: complete each listed pixel's emission once k_shadow has traced the
 // claimed sample slots.

@@ -517,6 +517,47 @@ def test_shadow_rays_through_several_transmissive_surfaces():
     assert diffuse.mean() > 0.3 and (want[diffuse, 4, :3] > 0).any()  # light reaches through the panes
 
 
+def test_light_samples_with_varying_draws_and_few_samples():
+    """Light samples are drawn where their shadow rays are traced, each from the RNG state advanced
+    past the samples before it, when every light sample takes the same number of draws.  Two other
+    forms remain and must give the same bits: lights whose samples take different draws (an area
+    light and a point light: samples drawn by k_nee_sample and by the camera pass), and fewer than
+    four samples per specular event (drawn by the camera pass)."""
+    base = P.SceneData.generate(A.PHX_SCENE_CORNELL, seed=1, width=32, height=32)
+    tris = base.triangles().copy()
+    mats = base.materials().copy()
+    mats[0]["metallic"], mats[0]["roughness"] = 0.3, 0.2  # specular events on the white walls
+    lights = np.zeros(2, dtype=base.lights().dtype)
+    lights[0] = base.lights()[0]
+    aux = np.array([lights[0]["aux"][c] for c in "xyzw"], np.float32).view(np.uint32)
+    light_tris = np.flatnonzero(tris["mat_index"] == 3)
+    aux[1], aux[2] = light_tris[0], len(light_tris)
+    for c, v in zip("xyzw", aux.view(np.float32)):
+        lights[0]["aux"][c] = v
+    lights[1]["kind"] = A.PHX_LIGHT_POINT
+    for c, v in zip("xyzw", (0.3, 0.8, 0.4, 1.0)):
+        lights[1]["position"][c] = v
+    for c, v in zip("xyzw", (1.5, 1.2, 0.9, 0.0)):
+        lights[1]["power"][c] = v
+    mixed = _scene_from_arrays(tris, mats, lights, base.scene.camera)
+    single = _scene_from_arrays(tris, mats, lights[:1].copy(), base.scene.camera)
+    for scene, ds in ((mixed, 16), (single, 2), (mixed, 3)):
+        args = P.ArgsList(width=40, height=40, photons_per_round=1 << 12, max_photon_bounces=8, grid_res=16,
+                          direct_samples=ds)
+        o = O.Oracle(scene)
+        with P.Renderer(args) as r:
+            r.set_scene(scene)
+            seed = 0x5EED + ds
+            r.trace_rays(seed)
+            got = np.stack([r.read(b) for b in ["HP_POS", "HP_NORMAL", "HP_THROUGHPUT", "HP_BASE_COLOR",
+                                                 "HP_DIRECT", "HP_EMISSION"]], axis=1)
+            r.iterate(2)
+            assert r.info().stack_overflows == 0
+        want = o.trace(args.width, args.height, seed, args.direct_samples)
+        assert assert_close(f"lights {len(scene.lights())} ds {ds}", got, want) == 1.0
+        assert (want[:, 4, :3] > 0).any()
+
+
 def test_state_and_argument_errors():
     scene, args = make("cornell")
     lib = A.load()
