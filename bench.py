@@ -230,6 +230,8 @@ def run_ours(a, cfg: dict) -> dict | None:
     args = make_args(cfg)
     if a.binary_bvh:
         args.flags = args.flags | 4  # PHX_F_BINARY_BVH
+    if a.leaf_size:
+        args.bvh_leaf_size = a.leaf_size
     scene = P.SceneData.generate(cfg["kind"], seed=1, width=args.width, height=args.height, detail=cfg["detail"])
     r = P.Renderer(args, device=local)
     r.set_scene(scene)
@@ -539,6 +541,7 @@ def main() -> int:
     ap.add_argument("--simple", action="store_true", help="one-thread-per-item kernels instead of lane refill")
     ap.add_argument("--persistent", action="store_true", help="lane-refill state-machine kernels")
     ap.add_argument("--binary-bvh", action="store_true", help="traverse child pairs instead of 4-wide nodes")
+    ap.add_argument("--leaf-size", type=int, default=0, help="triangles per leaf of the traversal tree (0: library default)")
     ap.add_argument("--autotune", action="store_true", help="run the library autotuner before timing")
     ap.add_argument("--shard", action="store_true",
                     help="one image over all GPUs (strong scaling) instead of one replica per GPU")
