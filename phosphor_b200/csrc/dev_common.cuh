@@ -167,7 +167,8 @@ PHX_HDI float4 random_unit_vector(Rng *rng) {
 }
 
 // random.h:48-62
-PHX_HDI float4 random_in_unit_hemisphere(Rng *rng, float4 normal) {
+// The same with the normal's frame (make_tbn of the normal) given by the caller.
+PHX_HDI float4 random_in_unit_hemisphere_tbn(Rng *rng, float4 normal, float4 t, float4 b) {
     normal.w = 0.0f;
     float r1 = random_float(rng);
     float r2 = random_float(rng);
@@ -175,9 +176,12 @@ PHX_HDI float4 random_in_unit_hemisphere(Rng *rng, float4 normal) {
     float st = sqrtf(r2);
     float ct = sqrtf(1.0f - r2);
     float4 hl = f4(st * pm_cosf(phi), st * pm_sinf(phi), ct, 0.0f);
-    float4 t, b;
-    make_tbn(normal, &t, &b);
     return normalize(hl.x * t + hl.y * b + hl.z * normal);
+}
+PHX_HDI float4 random_in_unit_hemisphere(Rng *rng, float4 normal) {
+    float4 t, b;
+    make_tbn(normal, &t, &b); // make_tbn ignores the normal's w, as the sampler does
+    return random_in_unit_hemisphere_tbn(rng, normal, t, b);
 }
 
 // ---- codecs: include/device/encoding.h:10-74 ---------------------------------------------------

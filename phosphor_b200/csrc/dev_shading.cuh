@@ -217,10 +217,10 @@ PHX_DI float4 safe_reflect(float4 d, float4 n, float4 gn) {
     return r;
 }
 
-PHX_DI float4 ggx_sample_vndf(Rng *rng, float4 normal, float4 gn, float4 view, float roughness) {
+// ggx_sample_vndf with the frame of `normal` (make_tbn) given by the caller.
+PHX_DI float4 ggx_sample_vndf_tbn(Rng *rng, float4 normal, float4 t, float4 b, float4 gn, float4 view,
+                                  float roughness) {
     float alpha = roughness * roughness;
-    float4 t, b;
-    make_tbn(normal, &t, &b);
     float4 vl = normalize(f4(dot(view, t), dot(view, b), dot(view, normal), 0.0f));
     float4 vh = normalize(f4(alpha * vl.x, alpha * vl.y, vl.z, 0.0f));
     float len_sq = vh.x * vh.x + vh.y * vh.y;
@@ -244,6 +244,11 @@ PHX_DI float4 ggx_sample_vndf(Rng *rng, float4 normal, float4 gn, float4 view, f
             return ne;
     }
     return normal;
+}
+PHX_DI float4 ggx_sample_vndf(Rng *rng, float4 normal, float4 gn, float4 view, float roughness) {
+    float4 t, b;
+    make_tbn(normal, &t, &b);
+    return ggx_sample_vndf_tbn(rng, normal, t, b, gn, view, roughness);
 }
 
 PHX_DI float smith_g1_ggx(float c, float alpha) {
@@ -293,7 +298,10 @@ struct BsdfSample {
 PHX_SHADE_BSDF BsdfSample sample_bsdf(Rng *rng, const ShadingContext &ctx, float4 sn, float4 gn, float4 view, IorStack *ior,
                               bool front) {
     BsdfSample s;
-    float4 h = ggx_sample_vndf(rng, sn, gn, view, ctx.roughness);
+    // one frame of the shading normal serves the microfacet sample and a diffuse direction
+    float4 tn, bn;
+    make_tbn(sn, &tn, &bn);
+    float4 h = ggx_sample_vndf_tbn(rng, sn, tn, bn, gn, view, ctx.roughness);
     float alpha = ctx.roughness * ctx.roughness;
     if (random_float(rng) < ctx.metallic) {
         s.dir = safe_reflect(-view, h, gn);
@@ -337,7 +345,7 @@ PHX_SHADE_BSDF BsdfSample sample_bsdf(Rng *rng, const ShadingContext &ctx, float
         s.event = BSDF_TRANSMIT;
         return s;
     }
-    s.dir = random_in_unit_hemisphere(rng, sn);
+    s.dir = random_in_unit_hemisphere_tbn(rng, sn, tn, bn);
     if (dot(s.dir, gn) <= 0.0f)
         s.dir = random_in_unit_hemisphere(rng, gn);
     s.throughput = ctx.base_color;
