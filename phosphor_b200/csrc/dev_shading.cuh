@@ -217,9 +217,12 @@ PHX_DI float4 safe_reflect(float4 d, float4 n, float4 gn) {
     return r;
 }
 
-// ggx_sample_vndf with the frame of `normal` (make_tbn) given by the caller.
+// ggx_sample_vndf with the frame of `normal` (make_tbn) given by the caller; *refl receives
+// reflect(-view, h) when the accepted attempt computed it (*has_refl), as it does unless every
+// attempt failed and h is the normal.
 PHX_DI float4 ggx_sample_vndf_tbn(Rng *rng, float4 normal, float4 t, float4 b, float4 gn, float4 view,
-                                  float roughness) {
+                                  float roughness, float4 *refl_out, bool *has_refl) {
+    *has_refl = false;
     float alpha = roughness * roughness;
     float4 vl = normalize(f4(dot(view, t), dot(view, b), dot(view, normal), 0.0f));
     float4 vh = normalize(f4(alpha * vl.x, alpha * vl.y, vl.z, 0.0f));
@@ -240,15 +243,19 @@ PHX_DI float4 ggx_sample_vndf_tbn(Rng *rng, float4 normal, float4 t, float4 b, f
         float4 nel = normalize(f4(alpha * nh.x, alpha * nh.y, fmaxf(0.0f, nh.z), 0.0f));
         float4 ne = normalize(nel.x * t + nel.y * b + nel.z * normal);
         float4 refl = reflect(-view, ne);
-        if (dot(refl, gn) >= 0.0f)
+        if (dot(refl, gn) >= 0.0f) {
+            *refl_out = refl;
+            *has_refl = true;
             return ne;
+        }
     }
     return normal;
 }
 PHX_DI float4 ggx_sample_vndf(Rng *rng, float4 normal, float4 gn, float4 view, float roughness) {
-    float4 t, b;
+    float4 t, b, refl;
+    bool has_refl;
     make_tbn(normal, &t, &b);
-    return ggx_sample_vndf_tbn(rng, normal, t, b, gn, view, roughness);
+    return ggx_sample_vndf_tbn(rng, normal, t, b, gn, view, roughness, &refl, &has_refl);
 }
 
 PHX_DI float smith_g1_ggx(float c, float alpha) {
@@ -301,10 +308,21 @@ PHX_SHADE_BSDF BsdfSample sample_bsdf(Rng *rng, const ShadingContext &ctx, float
     // one frame of the shading normal serves the microfacet sample and a diffuse direction
     float4 tn, bn;
     make_tbn(sn, &tn, &bn);
-    float4 h = ggx_sample_vndf_tbn(rng, sn, tn, bn, gn, view, ctx.roughness);
+    float4 hr;
+    bool has_hr;
+    float4 h = ggx_sample_vndf_tbn(rng, sn, tn, bn, gn, view, ctx.roughness, &hr, &has_hr);
+    // safe_reflect(-view, h, gn), reusing reflect(-view, h) from the microfacet sample
+    auto reflect_h = [&]() {
+        float4 r = has_hr ? hr : reflect(-view, h);
+        if (dot(r, gn) <= 0.0f) {
+            r = r - dot(r, gn) * gn;
+            r = normalize(r);
+        }
+        return r;
+    };
     float alpha = ctx.roughness * ctx.roughness;
     if (random_float(rng) < ctx.metallic) {
-        s.dir = safe_reflect(-view, h, gn);
+        s.dir = reflect_h();
         float cl = fmaxf(0.0f, dot(s.dir, sn));
         float g1 = smith_g1_ggx(cl, alpha);
         s.throughput = fresnel4(ctx.base_color, -view, h) * g1;
@@ -316,7 +334,7 @@ PHX_SHADE_BSDF BsdfSample sample_bsdf(Rng *rng, const ShadingContext &ctx, float
     float fr = fresnel_refracted(i1, i2, -view, h);
     float r_diel = random_float(rng);
     if (r_diel < fr) {
-        s.dir = safe_reflect(-view, h, gn);
+        s.dir = reflect_h();
         float cl = fmaxf(0.0f, dot(s.dir, sn));
         float g1 = smith_g1_ggx(cl, alpha);
         s.throughput = f4(g1, g1, g1, 0.0f);
@@ -328,7 +346,7 @@ PHX_SHADE_BSDF BsdfSample sample_bsdf(Rng *rng, const ShadingContext &ctx, float
         bool tir;
         float4 rf = refract(-view, h, i1, i2, &tir);
         if (tir) {
-            s.dir = safe_reflect(-view, h, gn);
+            s.dir = reflect_h();
             float cl = fmaxf(0.0f, dot(s.dir, sn));
             float g1 = smith_g1_ggx(cl, alpha);
             s.throughput = f4(g1, g1, g1, 0.0f);
