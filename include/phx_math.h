@@ -105,48 +105,36 @@ PHX_MATH_FN float pm_reduce_pio2(float x, int *quadrant) {
     return r;
 }
 
-PHX_MATH_FN float pm_sinf(float x) {
+/* sin and cos of x from one reduction: both polynomials, then the quadrant picks and signs them
+ * (selects, not branches, so that lanes in different quadrants stay together) */
+PHX_MATH_FN void pm_sincosf(float x, float *sn, float *cs) {
     if (!(fabsf(x) < 1.0e5f)) {
-        if (x != x || fabsf(x) == pm_bits_to_f(0x7f800000u))
-            return x - x; /* NaN */
+        if (x != x || fabsf(x) == pm_bits_to_f(0x7f800000u)) {
+            *sn = x - x; /* NaN */
+            *cs = x - x;
+            return;
+        }
     }
     int q;
     float r = pm_reduce_pio2(x, &q);
+    float s = pm_sin_kernel(r);
+    float c = pm_cos_kernel(r);
+    float a = (q & 1) ? c : s; /* sin: s, c, -s, -c in quadrants 0..3 */
+    float b = (q & 1) ? s : c; /* cos: c, -s, -c, s */
+    *sn = (q & 2) ? -a : a;
+    *cs = ((q + 1) & 2) ? -b : b;
+}
+
+PHX_MATH_FN float pm_sinf(float x) {
     float s, c;
-    switch (q) {
-    case 0:
-        return pm_sin_kernel(r);
-    case 1:
-        return pm_cos_kernel(r);
-    case 2:
-        s = pm_sin_kernel(r);
-        return -s;
-    default:
-        c = pm_cos_kernel(r);
-        return -c;
-    }
+    pm_sincosf(x, &s, &c);
+    return s;
 }
 
 PHX_MATH_FN float pm_cosf(float x) {
-    if (!(fabsf(x) < 1.0e5f)) {
-        if (x != x || fabsf(x) == pm_bits_to_f(0x7f800000u))
-            return x - x;
-    }
-    int q;
-    float r = pm_reduce_pio2(x, &q);
     float s, c;
-    switch (q) {
-    case 0:
-        return pm_cos_kernel(r);
-    case 1:
-        s = pm_sin_kernel(r);
-        return -s;
-    case 2:
-        c = pm_cos_kernel(r);
-        return -c;
-    default:
-        return pm_sin_kernel(r);
-    }
+    pm_sincosf(x, &s, &c);
+    return c;
 }
 
 /* ---- exp / log ---------------------------------------------------------------------------- */

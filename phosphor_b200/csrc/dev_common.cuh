@@ -163,7 +163,9 @@ PHX_HDI float4 random_unit_vector(Rng *rng) {
     float z = 2.0f * random_float(rng) - 1.0f;
     float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
     float phi = (2.0f * PI) * random_float(rng);
-    return f4(r * pm_cosf(phi), r * pm_sinf(phi), z, 0.0f);
+    float sp, cp;
+    pm_sincosf(phi, &sp, &cp);
+    return f4(r * cp, r * sp, z, 0.0f);
 }
 
 // random.h:48-62
@@ -175,7 +177,9 @@ PHX_HDI float4 random_in_unit_hemisphere_tbn(Rng *rng, float4 normal, float4 t, 
     float phi = (2.0f * PI) * r1;
     float st = sqrtf(r2);
     float ct = sqrtf(1.0f - r2);
-    float4 hl = f4(st * pm_cosf(phi), st * pm_sinf(phi), ct, 0.0f);
+    float sp, cp;
+    pm_sincosf(phi, &sp, &cp);
+    float4 hl = f4(st * cp, st * sp, ct, 0.0f);
     return normalize(hl.x * t + hl.y * b + hl.z * normal);
 }
 PHX_HDI float4 random_in_unit_hemisphere(Rng *rng, float4 normal) {

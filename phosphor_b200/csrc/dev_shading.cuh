@@ -117,7 +117,8 @@ PHX_DI float4 sample_texture(const SceneDesc &sc, u32 index, float ux, float uy)
 PHX_SHADE_TEX float4 sample_texture_uv(const SceneDesc &sc, u32 mat_index, u32 tex_index, float ux, float uy, u32 slot) {
     const phx_uv_transform *t = &sc.uvt[mat_index].diff + slot;
     float sx = ux * t->uv_scale.x, sy = uy * t->uv_scale.y;
-    float c = pm_cosf(t->uv_rotation), s = pm_sinf(t->uv_rotation);
+    float c, s;
+    pm_sincosf(t->uv_rotation, &s, &c);
     float rx = c * sx - s * sy, ry = s * sx + c * sy;
     return sample_texture(sc, tex_index, rx + t->uv_offset.x, ry + t->uv_offset.y);
 }
@@ -235,8 +236,10 @@ PHX_DI float4 ggx_sample_vndf_tbn(Rng *rng, float4 normal, float4 t, float4 b, f
         float u2 = random_float(rng);
         float r = sqrtf(u1);
         float phi = (2.0f * PI) * u2;
-        float t1 = r * pm_cosf(phi);
-        float t2 = r * pm_sinf(phi);
+        float sp, cp;
+        pm_sincosf(phi, &sp, &cp);
+        float t1 = r * cp;
+        float t2 = r * sp;
         t2 = (1.0f - s) * sqrtf(fmaxf(0.0f, 1.0f - t1 * t1)) + s * t2;
         float nz2 = fmaxf(0.0f, 1.0f - t1 * t1 - t2 * t2);
         float4 nh = t1 * T1 + t2 * T2 + sqrtf(nz2) * vh;
@@ -486,7 +489,9 @@ PHX_SHADE_LIGHT void sample_light(Rng *rng, const SceneDesc &sc, float4 *origin,
         float ct = 1.0f - r1 * (1.0f - co);
         float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
         float phi = (2.0f * PI) * r2;
-        float4 ld = f4(st * pm_cosf(phi), st * pm_sinf(phi), ct, 0.0f);
+        float sp, cp;
+        pm_sincosf(phi, &sp, &cp);
+        float4 ld = f4(st * cp, st * sp, ct, 0.0f);
         float4 t, b;
         float4 ldir = normalize(f4(L.direction));
         make_tbn(ldir, &t, &b);
@@ -499,7 +504,9 @@ PHX_SHADE_LIGHT void sample_light(Rng *rng, const SceneDesc &sc, float4 *origin,
         float radius = sc.scene_radius;
         float r1 = radius * sqrtf(random_float(rng));
         float r2 = (2.0f * PI) * random_float(rng);
-        float4 disk = r1 * (pm_cosf(r2) * f4(L.tangent) + pm_sinf(r2) * f4(L.bitangent));
+        float s2, c2;
+        pm_sincosf(r2, &s2, &c2);
+        float4 disk = r1 * (c2 * f4(L.tangent) + s2 * f4(L.bitangent));
         *dir = f4(L.direction);
         *origin = center - f4(L.direction) * 2.0f * radius + disk;
         *power = f4(L.power) * PI * radius * radius;
@@ -722,7 +729,8 @@ PHX_DI void make_ray(const phx_camera_params &cam, u32 px, u32 py, u32 width, u3
     if (cam.defocus_angle > 0.0f) {
         float r1 = sqrtf(random_float(rng));
         float r2 = (2.0f * PI) * random_float(rng);
-        float c = pm_cosf(r2), sn = pm_sinf(r2);
+        float c, sn;
+        pm_sincosf(r2, &sn, &c);
         disk = r1 * (c * f4(cam.defocus_disk_u) + sn * f4(cam.defocus_disk_v));
     }
     *origin = f4(cam.position) + disk;
