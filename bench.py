@@ -50,10 +50,10 @@ CONFIGS = {
 METRIC = "Mphotons/s"
 # dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu capture of the full-size
 # workload (profiles/dram_traffic_caustic_1024.md)
-# (a stage's kernels summed; the shadow stage: k_nee_sample, k_shadow, k_shadow_spec, k_nee_resolve,
-# k_spec_resolve)
-NCU_TRAFFIC = {"caustic": {"trace": 1_355_299_328, "shadow": 2_066_197_504, "emit": 383_891_200,
-                           "gather": 290_075_136}}
+# (a stage's kernels summed; the shadow stage: k_shadow, k_nee_resolve, k_spec_resolve — k_nee_sample
+# does not run for scenes whose light samples all take the same RNG draws)
+NCU_TRAFFIC = {"caustic": {"trace": 939_781_376, "shadow": 991_296_512, "emit": 465_910_784,
+                           "gather": 306_744_576}}
 ALGO_STAGES = ["trace", "shadow", "emit", "emit_scan", "hash", "cell_scan", "sort", "records", "gather"]
 
 
@@ -193,12 +193,14 @@ def algorithmic_bytes(stage: str, P: int, Ne: int, Ns: int, C: int, scene_bytes:
     stage must read or write once, plus the scene geometry for the traversal stages.  S = specular
     NEE samples the camera pass deferred."""
     return {
-        # camera pass: the hit point (96 B) and the NEE stash (32 B) per pixel; per deferred
-        # specular sample its ray, weight, origin and pixel (52 B)
-        "trace": 96 * P + 32 * P + 52 * S + scene_bytes,
-        # NEE samples written (32 B), read and replaced by the shadow pass (32 + 16 B), summed (16 B);
-        # specular samples read (52 B), replaced (16 B) and summed (16 B)
-        "shadow": 96 * P * ds + 48 * P + 84 * S + scene_bytes,
+        # camera pass: the hit point (96 B) and the NEE stash (20 B) per pixel; per deferred
+        # specular sample its header and pixel (20 B) and its share of the event's 64-byte record
+        "trace": 96 * P + 20 * P + 20 * S + 64 * S // ds + scene_bytes,
+        # each sample drawn in the shadow pass from the pixel's stash (pixel reads: position, stash,
+        # base colour, emission, throughput: 84 B; direct written: 16 B), its contribution written
+        # and summed (16 + 16 B); a specular sample reads its header, pixel and event record share,
+        # its contribution is written and summed (16 + 16 B)
+        "shadow": 32 * P * ds + 100 * P + 52 * S + 64 * S // ds + scene_bytes,
         "emit": 24 * Ns + scene_bytes,
         "emit_scan": 8 * Ne + 48 * Ns,
         "hash": 16 * Ns + 4 * Ns + 4 * C + 8 * Ns,
