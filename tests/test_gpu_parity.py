@@ -328,6 +328,29 @@ def test_batch_retired_scene_stops_and_others_continue():
     batch.close()
 
 
+def test_batch_with_scenes_sharing_warps():
+    """Odd pixel counts at 16 samples per pixel: a scene's pixels and sample slots end inside a
+    warp, so warps of every per-pixel and per-sample kernel straddle two scenes, and each scene
+    alone ends with a partial warp; the batch still equals every scene alone."""
+    made = []
+    for kind, w, h, seed, detail in [(A.PHX_SCENE_CAUSTIC, 13, 11, 4, 0), (A.PHX_SCENE_CORNELL, 9, 7, 3, 0),
+                                     (A.PHX_SCENE_ATRIUM, 15, 9, 5, 16), (A.PHX_SCENE_CAUSTIC, 7, 5, 6, 0)]:
+        scene = P.SceneData.generate(kind, seed=seed, width=w, height=h, detail=detail)
+        args = P.ArgsList(width=w, height=h, photons_per_round=1 << 12, max_photon_bounces=8, grid_res=16,
+                          seed=seed, direct_samples=16)
+        made.append((scene, args))
+    batch = P.Batch([s for s, _ in made], [a for _, a in made])
+    batch.iterate(3, graph=True)
+    for i, (scene, args) in enumerate(made):
+        with P.Renderer(args) as r:
+            r.set_scene(scene)
+            r.iterate(3)
+            for buf in ["FLUX", "PHOTON_WEIGHT", "RADIANCE", "HP_DIRECT", "HP_EMISSION"]:
+                assert np.array_equal(batch.read(i, buf).view(np.uint32), r.read(buf).view(np.uint32)), (i, buf)
+            assert r.info().stack_overflows == 0
+    batch.close()
+
+
 PIPE_BUFS = ["FLUX", "PHOTON_WEIGHT", "RADIANCE", "HP_POS", "HP_DIRECT", "HP_EMISSION", "PHOTON_POS",
              "SORTED_POS", "SORT_PERM", "CELL_START"]
 
