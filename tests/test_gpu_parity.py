@@ -351,6 +351,46 @@ def test_batch_with_scenes_sharing_warps():
     batch.close()
 
 
+def test_material_change_recaptures_for_the_new_shadow_kind():
+    """A scene whose every material blocks shadow rays replays graphs with the any-hit shadow
+    kernel; making its water transmissive again (set_materials) must bring back the listing
+    traversal for the next replays.  Graph replays before and after the change equal plain rounds
+    (launched afresh each time) of a second context taken through the same changes, and both
+    differ from the rounds the opaque water alone would give."""
+    scene, args = make("caustic")
+    view = scene.materials()
+    glass = view.copy()
+    water = int(np.argmax(glass["transmission"]))
+    assert glass["transmission"][water] > 0.5
+    opaque = glass.copy()
+    opaque["transmission"][water] = 0.0
+    bufs = ["FLUX", "PHOTON_WEIGHT", "RADIANCE", "HP_DIRECT", "HP_EMISSION"]
+    view[:] = opaque
+    try:
+        a, b, c = P.Renderer(args), P.Renderer(args), P.Renderer(args)
+        for r in (a, b, c):
+            r.set_scene(scene)  # the scene's arrays are copied here
+    finally:
+        view[:] = glass
+    try:
+        a.iterate(2)
+        for _ in range(2):
+            b.round()
+        c.iterate(5)
+        a.set_materials(glass)
+        b.set_materials(glass)
+        a.iterate(3)
+        for _ in range(3):
+            b.round()
+        for buf in bufs:
+            assert np.array_equal(a.read(buf).view(np.uint32), b.read(buf).view(np.uint32)), buf
+        assert any(not np.array_equal(a.read(buf).view(np.uint32), c.read(buf).view(np.uint32)) for buf in bufs)
+        assert a.info().stack_overflows == 0
+    finally:
+        for r in (a, b, c):
+            r.close()
+
+
 PIPE_BUFS = ["FLUX", "PHOTON_WEIGHT", "RADIANCE", "HP_POS", "HP_DIRECT", "HP_EMISSION", "PHOTON_POS",
              "SORTED_POS", "SORT_PERM", "CELL_START"]
 
