@@ -177,6 +177,23 @@ PHX_DI float box1(float nx, float fx, float ny, float fy, float nz, float fz, fl
     return tn <= tf ? tn : __int_as_float(0x7f800000);
 }
 
+// The slab tests' inverse direction component 1/dc, except that the +-inf of a zero component
+// becomes +-1e30 while the origin's coordinate oc is below 1e4 in magnitude.  A ray with dc = 0
+// keeps the coordinate oc.  With +-inf, every plane on the same side of zero as oc gave
+// inf - inf = NaN, which the slab tests ignore: that axis pruned nothing, and an axis-aligned ray
+// visited most of the tree — 62,533 steps for one photon of the 1920x1080 atrium workload emitted
+// straight down, direction (0, 0, -1), from its point light: 26-40 ms added to about one round in
+// ten.  With 1e30 a slab's distances are (plane - oc) * 1e30 up to a rounding
+// of |oc| * 2^-24 * 1e30, so their signs are exact for every plane farther than 6e-4 from oc, as
+// is every plane of a box holding a triangle the ray can hit (triangle boxes are widened by 1e-3
+// and the ray's coordinate must lie within the triangle's range).  A box that oc lies outside of
+// gets two distances of one sign, at least ~1e27 in magnitude, and is pruned.  NaN and finite
+// inverses are unchanged.
+PHX_DI float slab_inv(float dc, float oc) {
+    const float r = 1.0f / dc;
+    return (fabsf(r) == __int_as_float(0x7f800000) && fabsf(oc) < 1e4f) ? copysignf(1e30f, r) : r;
+}
+
 PHX_DI void sort2(float &ta, i32 &ra, float &tb, i32 &rb) {
     if (tb < ta) {
         float t = ta;
@@ -254,7 +271,7 @@ PHX_DI bool intersect_t(const SceneDesc &sc, float4 o, float4 d, float t_min, fl
     constexpr bool LISTED = !std::is_same<LIST, NoHitList>::value;
     float opaque = t_max; // LISTED: nearest opaque hit so far
     constexpr i32 POP = 0x7fffffff;
-    const float ix = 1.0f / d.x, iy = 1.0f / d.y, iz = 1.0f / d.z;
+    const float ix = slab_inv(d.x, o.x), iy = slab_inv(d.y, o.y), iz = slab_inv(d.z, o.z);
     const float oix = o.x * ix, oiy = o.y * iy, oiz = o.z * iz;
     // 4-wide nodes: offsets of the entry-plane rows {minx, maxx, miny, maxy, minz, maxz}
     const int px = ix >= 0.0f ? 0 : 1, py = iy >= 0.0f ? 2 : 3, pz = iz >= 0.0f ? 4 : 5;

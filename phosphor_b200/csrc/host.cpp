@@ -262,7 +262,9 @@ bool bvh_build_sah(const phx_triangle *tris, uint32_t n, const std::vector<uint3
         float x = h[0] - l[0], y = h[1] - l[1], z = h[2] - l[2];
         return x * y + y * z + z * x;
     };
-    constexpr int NB = 32;
+    // centroid bins per axis: 128 for ranges of 256 triangles or more (shadow stage 7.18 -> 7.10 ms on
+    // the caustic workload, 3.19 -> 3.09 ms on the atrium one, against 32 everywhere), 32 below
+    constexpr int NB = 128;
     out.cnodes.clear();
     out.cnodes.reserve((size_t)n * 16);
     out.trirec.assign((size_t)n * 12, 0.0f);
@@ -295,6 +297,7 @@ bool bvh_build_sah(const phx_triangle *tris, uint32_t n, const std::vector<uint3
             }
         int32_t ref;
         // choose a split
+        const int nb = cnt >= 256 ? NB : 32;
         float best = 1e30f;
         int bax = -1, bbin = 0;
         if (cnt > 1) {
@@ -304,14 +307,14 @@ bool bvh_build_sah(const phx_triangle *tris, uint32_t n, const std::vector<uint3
                     continue;
                 int bc[NB] = {0};
                 float bl[NB][3], bh[NB][3];
-                for (int k = 0; k < NB; k++)
+                for (int k = 0; k < nb; k++)
                     for (int j = 0; j < 3; j++) {
                         bl[k][j] = 1e30f;
                         bh[k][j] = -1e30f;
                     }
-                const float sc = NB / ext;
+                const float sc = nb / ext;
                 for (uint32_t i = b; i < e; i++) {
-                    int k = std::min(NB - 1, (int)((P[i].c[a] - clo[a]) * sc));
+                    int k = std::min(nb - 1, (int)((P[i].c[a] - clo[a]) * sc));
                     bc[k]++;
                     for (int j = 0; j < 3; j++) {
                         bl[k][j] = std::min(bl[k][j], P[i].lo[j]);
@@ -322,7 +325,7 @@ bool bvh_build_sah(const phx_triangle *tris, uint32_t n, const std::vector<uint3
                 int rn[NB];
                 float rl[3] = {1e30f, 1e30f, 1e30f}, rh[3] = {-1e30f, -1e30f, -1e30f};
                 int acc = 0;
-                for (int k = NB - 1; k > 0; k--) {
+                for (int k = nb - 1; k > 0; k--) {
                     acc += bc[k];
                     for (int j = 0; j < 3; j++) {
                         rl[j] = std::min(rl[j], bl[k][j]);
@@ -333,7 +336,7 @@ bool bvh_build_sah(const phx_triangle *tris, uint32_t n, const std::vector<uint3
                 }
                 float ll[3] = {1e30f, 1e30f, 1e30f}, lh[3] = {-1e30f, -1e30f, -1e30f};
                 int ln = 0;
-                for (int k = 1; k < NB; k++) {
+                for (int k = 1; k < nb; k++) {
                     ln += bc[k - 1];
                     for (int j = 0; j < 3; j++) {
                         ll[j] = std::min(ll[j], bl[k - 1][j]);
@@ -351,7 +354,10 @@ bool bvh_build_sah(const phx_triangle *tris, uint32_t n, const std::vector<uint3
             }
         }
         const float parea = area(lo, hi);
-        const bool make_leaf = cnt == 1 || (cnt <= max_leaf && (bax < 0 || 1.0f + best / parea >= (float)cnt));
+#ifndef PHX_SAH_CT
+#define PHX_SAH_CT 1.0f
+#endif
+        const bool make_leaf = cnt == 1 || (cnt <= max_leaf && (bax < 0 || PHX_SAH_CT + best / parea >= (float)cnt));
         if (make_leaf && cnt <= max_leaf) {
             uint32_t first = next_tri;
             // keep triangles of a leaf in reference-rank order (irrelevant for results, stable)
@@ -371,9 +377,9 @@ bool bvh_build_sah(const phx_triangle *tris, uint32_t n, const std::vector<uint3
         }
         uint32_t mid;
         if (bax >= 0) {
-            const float ext = chi[bax] - clo[bax], sc = NB / ext;
+            const float ext = chi[bax] - clo[bax], sc = nb / ext;
             auto it = std::partition(P.begin() + b, P.begin() + e, [&](const Prim &p) {
-                return std::min(NB - 1, (int)((p.c[bax] - clo[bax]) * sc)) < bbin;
+                return std::min(nb - 1, (int)((p.c[bax] - clo[bax]) * sc)) < bbin;
             });
             mid = (uint32_t)(it - P.begin());
             if (mid == b || mid == e)
