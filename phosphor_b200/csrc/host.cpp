@@ -354,10 +354,7 @@ bool bvh_build_sah(const phx_triangle *tris, uint32_t n, const std::vector<uint3
             }
         }
         const float parea = area(lo, hi);
-#ifndef PHX_SAH_CT
-#define PHX_SAH_CT 1.0f
-#endif
-        const bool make_leaf = cnt == 1 || (cnt <= max_leaf && (bax < 0 || PHX_SAH_CT + best / parea >= (float)cnt));
+        const bool make_leaf = cnt == 1 || (cnt <= max_leaf && (bax < 0 || 1.0f + best / parea >= (float)cnt));
         if (make_leaf && cnt <= max_leaf) {
             uint32_t first = next_tri;
             // keep triangles of a leaf in reference-rank order (irrelevant for results, stable)

@@ -559,6 +559,56 @@ def _glass_panes_scene():
     return _scene_from_arrays(tris, mats, lights, base.scene.camera)
 
 
+def _pcg_draw(v, k):
+    """Draw k of the PCG stream pcg_seed(v) (random.h:16-34), as a u32."""
+    m = 0xFFFFFFFF
+    state = ((2891336453 + v) * 747796405 + 2891336453) & m
+    for _ in range(k + 1):
+        old = state
+        state = (state * 747796405 + 2891336453) & m
+    return (((old >> ((old >> 28) + 4)) ^ old) * 277803737) & m
+
+
+@pytest.mark.parametrize("v", [37166213, 7983376])
+def test_axis_aligned_photons(v):
+    """A photon leaving a point light along -z or +z, its x and y direction components exactly
+    zero: draw 1 of its stream (the unit-sphere sample's z, after the light choice) is 7 or
+    2^32 - 86, so z = 2u - 1 rounds to -1 or +1.  The traversal's x and y slabs then use a finite
+    stand-in for 1/0; the -z photon still finds the back wall of the box and the bounces after it,
+    the +z one leaves through the open front, and every photon equals the oracle's."""
+    t = 5
+    w = _pcg_draw(v, 1)
+    assert w < 64 or w >= (1 << 32) - 128
+    base = P.SceneData.generate(A.PHX_SCENE_CORNELL, seed=1, width=16, height=16)
+    tris = base.triangles()[:10].copy()  # the box without its ceiling light; back wall at z = 0
+    mats = base.materials()[:3].copy()
+    lights = np.zeros(1, dtype=base.lights().dtype)
+    lights[0]["kind"] = A.PHX_LIGHT_POINT
+    for c, x in zip("xyz", (0.3, 0.6, 0.5)):
+        lights[0]["position"][c] = x
+        lights[0]["power"][c] = 1.0
+    scene = _scene_from_arrays(tris, mats, lights, base.scene.camera)
+    args = P.ArgsList(width=16, height=16, photons_per_round=64, max_photon_bounces=4, grid_res=8, seed=1,
+                      direct_samples=4)
+    seed = (v - t) & 0xFFFFFFFF  # photon t's stream is pcg_seed(seed + t)
+    o = O.Oracle(scene)
+    ocounts, opos, opower, odir = o.emit(0, args.photons_per_round, args.max_photon_bounces, seed)
+    first = int(np.sum(ocounts[:t]))
+    if w < 64:  # straight at the back wall
+        assert ocounts[t] >= 1 and np.array_equal(opos[first, :3], np.array([0.3, 0.6, 0.0], np.float32))
+    else:
+        assert ocounts[t] == 0
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        n = r.emit_photons(seed)
+        assert n == len(opos)
+        assert np.array_equal(r.read("EMIT_COUNT"), ocounts)
+        assert np.array_equal(r.read("PHOTON_POWER"), opower)
+        assert np.array_equal(r.read("PHOTON_DIR"), odir)
+        assert np.array_equal(r.read("PHOTON_POS").view(np.uint32), np.asarray(opos, np.float32).view(np.uint32))
+        assert r.info().stack_overflows == 0
+
+
 def test_shadow_rays_through_several_transmissive_surfaces():
     """Shadow rays that cross more transmissive surfaces than one traversal lists go on with
     closest-hit queries past the listed ones; hit points (direct light included) stay bit-exact."""
