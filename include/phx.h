@@ -431,6 +431,27 @@ PHX_API int phx_selftest_lookback_timeout(int device, uint32_t n, uint32_t *err_
  * Returns PHX_E_TIMEOUT if a bounded look-back wait gave up (results then invalid). */
 PHX_API int phx_scan_noalloc(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *total, uint64_t stream);
 
+/* ---- denoise filters (denoise/filters_gpu.py:9-86) ----------------------------------------------
+ * The reference denoiser's three OpenCL image kernels, replacing mean_filter_gpu /
+ * median_filter_gpu / gaussian_filter_gpu's kernel launches (filters_gpu.py:128-161).  `in` is an
+ * (height, width, 3) int32 image and `out` an (height, width, 3) float32 one, both host memory;
+ * each output value is taken over the window [x-k, x+k] x [y-k, y+k] clamped to the image (border
+ * windows shrink), summing in the kernels' order (x outer, y inner) with one rounding per float
+ * operation: the reference kernels' results bit for bit.
+ *   mean:      window sum / window pixel count;
+ *   median:    window median, the mean of the two middle values for an even count (k <= 2, as
+ *              the reference raises for k > 2: PHX_E_INVALID);
+ *   weighted:  sum of value * weights[(yy - y + k) * (2k + 1) + (xx - x + k)]; `weights` holds
+ *              (2k+1)^2 floats (gaussian_filter_gpu passes the normalised Gaussian).
+ * k <= 32.  Synchronous on a stream of its own on the current device.  kernel_ms, if not NULL,
+ * receives the filter kernel's CUDA-event time (copies excluded). */
+PHX_API int phx_mean_filter(const int32_t *in, float *out, uint32_t width, uint32_t height, uint32_t k,
+                            float *kernel_ms);
+PHX_API int phx_median_filter(const int32_t *in, float *out, uint32_t width, uint32_t height, uint32_t k,
+                              float *kernel_ms);
+PHX_API int phx_weighted_filter(const int32_t *in, float *out, const float *weights, uint32_t width, uint32_t height,
+                                uint32_t k, float *kernel_ms);
+
 PHX_API const char *phx_last_error(void);
 PHX_API const char *phx_version(void);
 

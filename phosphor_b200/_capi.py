@@ -176,6 +176,9 @@ PROTOTYPES = [
     ("phx_get_stream", C.c_uint64, [VP]),
     ("phx_selftest_lookback_timeout", C.c_int, [C.c_int, C.c_uint32, C.POINTER(C.c_uint32)]),
     ("phx_scan_noalloc", C.c_int, [VP, VP, C.c_uint32, VP, C.c_uint64]),
+    ("phx_mean_filter", C.c_int, [VP, VP, C.c_uint32, C.c_uint32, C.c_uint32, VP]),
+    ("phx_median_filter", C.c_int, [VP, VP, C.c_uint32, C.c_uint32, C.c_uint32, VP]),
+    ("phx_weighted_filter", C.c_int, [VP, VP, VP, C.c_uint32, C.c_uint32, C.c_uint32, VP]),
     ("phx_batch_set_active", C.c_int, [VP, C.c_uint32, C.c_int]),
     ("phx_shard", C.c_int, [VP, C.c_uint32, C.c_uint32]),
     ("phx_shard_begin", C.c_int, [VP, C.POINTER(C.c_uint32)]),

@@ -466,4 +466,32 @@ PHX_API int phx_scan_noalloc(const uint32_t *in, uint32_t *out, uint32_t n, uint
     });
 }
 
+static int filter_entry(int mode, const int32_t *in, float *out, const float *weights, uint32_t width,
+                        uint32_t height, uint32_t k, float *kernel_ms) {
+    return guard([&]() -> int {
+        std::string msg;
+        const int rc = denoise_filter(mode, in, out, weights, width, height, k, kernel_ms, msg);
+        if (rc == 1)
+            return fail(PHX_E_INVALID, msg);
+        if (rc == 3)
+            return fail(PHX_E_CUDA, msg);
+        return PHX_OK;
+    });
+}
+
+PHX_API int phx_mean_filter(const int32_t *in, float *out, uint32_t width, uint32_t height, uint32_t k,
+                            float *kernel_ms) {
+    return filter_entry(0, in, out, nullptr, width, height, k, kernel_ms);
+}
+
+PHX_API int phx_median_filter(const int32_t *in, float *out, uint32_t width, uint32_t height, uint32_t k,
+                              float *kernel_ms) {
+    return filter_entry(1, in, out, nullptr, width, height, k, kernel_ms);
+}
+
+PHX_API int phx_weighted_filter(const int32_t *in, float *out, const float *weights, uint32_t width, uint32_t height,
+                                uint32_t k, float *kernel_ms) {
+    return filter_entry(2, in, out, weights, width, height, k, kernel_ms);
+}
+
 } // extern "C"

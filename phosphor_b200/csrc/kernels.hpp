@@ -101,6 +101,9 @@ int selftest_lookback_timeout(int device, u32 n, u32 *err_out);
 // exclusive scan with its scratch in a static device array (no allocation); synchronous.
 // returns 0 ok, 1 too large, 3 CUDA error, 4 look-back timeout (message in err)
 int scan_noalloc(const u32 *in, u32 *out, u32 n, u32 *total, cudaStream_t st, std::string &err);
+// k_denoise.cu: mode 0 mean, 1 median, 2 weighted; 0 = ok, 1 = invalid argument, 3 = CUDA error
+int denoise_filter(int mode, const int32_t *in, float *out, const float *weights, uint32_t width, uint32_t height,
+                   uint32_t k, float *kernel_ms, std::string &msg);
 
 // stable LSD radix sort of (key, canonical index) by key; n read from device *n_dev (<= n_max)
 size_t radix_scratch_bytes(u64 n_max, u32 key_bits);
