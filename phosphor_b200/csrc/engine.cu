@@ -615,7 +615,7 @@ void Engine::enq_gather_r(RoundSet &R, cudaStream_t s) {
     ev(ST_GATHER, false, s);
     const u32 *order = nullptr;
     if (tune.gather_sorted && pix_key_bits) {
-        launch_pixel_keys(lc(R), R.hp[0], R.hp[5], pk_keys.as<u32>(), s);
+        launch_pixel_keys(lc(R), R.hp[0], R.hp[5], pix_key_bits, pk_keys.as<u32>(), s);
         launch_radix_sort(pk_keys.as<u32>(), pk_t0.as<u32>(), pk_t1.as<u32>(), pk_v0.as<u32>(), pk_v1.as<u32>(),
                           &pix_order, d_npix.as<u32>(), total_pixels, pix_key_bits, pk_scr.p, d_err.as<u32>(), s);
         order = pix_order;

@@ -146,14 +146,16 @@ __global__ void __launch_bounds__(128, PHX_GATHER_MINB) k_gather(LaunchCtx lc, G
 
 // Pixels whose hit points share a photon-grid cell (and an octant of it) visit the same cells and
 // skip the same ones, so gathering them in one warp keeps its lanes in step and lets them share
-// every photon record load.  Each pixel's own computation does not change.
+// every photon record load.  Pixels without a diffuse hit point (nothing to gather) sort last.
+// Each pixel's own computation does not change.
 __global__ void __launch_bounds__(256) k_pixel_keys(LaunchCtx lc, const float4 *hp_pos, const float4 *hp_emission,
-                                                    u32 *keys) {
+                                                    u32 key_bits, u32 *keys) {
     const u32 gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= lc.total_pixels)
         return;
-    u32 key = 0;
+    u32 key = key_bits >= 32 ? 0xffffffffu : (1u << key_bits) - 1u;
     if (hp_emission[gid].w == 1.0f) {
+        key = 0; // outside the grid
         const u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gid);
         const SceneDesc &sc = lc.scenes[s];
         const float4 p = hp_pos[gid];
@@ -169,10 +171,10 @@ __global__ void __launch_bounds__(256) k_pixel_keys(LaunchCtx lc, const float4 *
     keys[gid] = key;
 }
 
-void launch_pixel_keys(const LaunchCtx &lc, const float4 *hp_pos, const float4 *hp_emission, u32 *keys,
+void launch_pixel_keys(const LaunchCtx &lc, const float4 *hp_pos, const float4 *hp_emission, u32 key_bits, u32 *keys,
                        cudaStream_t st) {
     if (lc.total_pixels)
-        k_pixel_keys<<<(lc.total_pixels + 255) / 256, 256, 0, st>>>(lc, hp_pos, hp_emission, keys);
+        k_pixel_keys<<<(lc.total_pixels + 255) / 256, 256, 0, st>>>(lc, hp_pos, hp_emission, key_bits, keys);
 }
 
 void launch_gather(const LaunchCtx &lc, const GatherBufs &g, int block, cudaStream_t st) {

@@ -133,7 +133,7 @@ struct GatherBufs {
 void launch_gather(const LaunchCtx &lc, const GatherBufs &g, int block, cudaStream_t st);
 // Per pixel a sort key that groups hit points by photon-grid cell: ((cell_base + cell) << 3 | octant
 // of the point inside its cell), 0 for pixels without a diffuse hit point.
-void launch_pixel_keys(const LaunchCtx &lc, const float4 *hp_pos, const float4 *hp_emission, u32 *keys,
+void launch_pixel_keys(const LaunchCtx &lc, const float4 *hp_pos, const float4 *hp_emission, u32 key_bits, u32 *keys,
                        cudaStream_t st);
 
 // adjoint (single scene): gather adjoint, camera / photon path replays, helpers
