@@ -161,7 +161,9 @@ def time_batched(specs, rounds: int, device: int = 0) -> float:
 
 
 TAIL_CONCURRENT = 2  # active scenes at or below which the camera and photon passes run concurrently
-PIPELINE_ROUNDS = 8  # rounds per captured graph, their passes overlapped (phx_tuning.pipeline_rounds)
+# rounds per captured graph, their passes overlapped (phx_tuning.pipeline_rounds); measured on the
+# 16-scene batch: 4.74 s with 8, 4.99 s with 12 and 5.06-5.47 s with 16
+PIPELINE_ROUNDS = 8
 
 
 def time_batched_schedule(specs, r_star: list[int], device: int = 0, pipeline: int = PIPELINE_ROUNDS) -> float:
