@@ -54,10 +54,10 @@ void launch_compact(const LaunchCtx &lc, const GridBufs &g, cudaStream_t st) {
 
 // ---- hash (hash_photons.cl:4-13) ---------------------------------------------------------------
 // Canonical photon i belongs to the scene whose photon range [offsets[emit_base], ...) holds it.
-__global__ void __launch_bounds__(256) k_hash(LaunchCtx lc, GridBufs g, const u32 *n_dev, u64 n_max) {
-    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_max || i >= *n_dev)
-        return;
+// The grid is sized for the photon capacity (photons_per_round * max_bounces, often 10-100x the
+// photons stored), so the threads stride over the stored ones instead of one block per 256 slots
+// of capacity: the empty blocks alone took most of the stage (atrium workload).
+PHX_DI void hash_one(const LaunchCtx &lc, const GridBufs &g, u64 i) {
     u32 s = 0;
     if (lc.n_scenes > 1) {
         u32 lo = 0, hi = lc.n_scenes;
@@ -77,10 +77,22 @@ __global__ void __launch_bounds__(256) k_hash(LaunchCtx lc, GridBufs g, const u3
     atomicAdd(&g.cell_count[key], 1u);
 }
 
+__global__ void __launch_bounds__(256) k_hash(LaunchCtx lc, GridBufs g, const u32 *n_dev, u64 n_max) {
+    const u64 n = min((u64)*n_dev, n_max);
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+        hash_one(lc, g, i);
+}
+
+// blocks for a grid-stride loop over at most n_max items: enough to fill every SM several times
+static unsigned stride_blocks(u64 n_max, unsigned threads) {
+    const u64 need = (n_max + threads - 1) / threads, cap = (u64)(g_sm_count > 0 ? g_sm_count : 148) * 16;
+    return (unsigned)(need < cap ? (need > 0 ? need : 1) : cap);
+}
+
 void launch_hash(const LaunchCtx &lc, const GridBufs &g, const u32 *n_dev, u64 n_max, cudaStream_t st) {
     if (n_max == 0)
         return;
-    k_hash<<<(unsigned)((n_max + 255) / 256), 256, 0, st>>>(lc, g, n_dev, n_max);
+    k_hash<<<stride_blocks(n_max, 256), 256, 0, st>>>(lc, g, n_dev, n_max);
 }
 
 // ---- decoupled look-back exclusive scan --------------------------------------------------------
@@ -104,15 +116,23 @@ PHX_DI u64 peek(u64 *status) {
     return a.load(cuda::memory_order_acquire);
 }
 
+// n_dyn (optional): the length is only n' = min(n, dyn_mul * ceil(*n_dyn / dyn_div)), read on the
+// device (a graph replays one launch shape for every round); tiles past n' return at once, and
+// since a tile only waits on lower ones, no tile waits on them.
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan(const u32 *__restrict__ in, u32 *__restrict__ out, u64 n,
-                                                      u32 *tile_counter, u64 *status, u32 *total, u32 *err) {
+                                                      u32 *tile_counter, u64 *status, u32 *total, u32 *err,
+                                                      const u32 *n_dyn, u32 dyn_div, u32 dyn_mul) {
     __shared__ u32 s_tile;
     __shared__ u32 s_warp[SCAN_THREADS / 32];
     __shared__ u32 s_prefix;
     if (threadIdx.x == 0)
         s_tile = atomicAdd(tile_counter, 1u);
+    if (n_dyn)
+        n = min(n, (u64)dyn_mul * (((u64)*n_dyn + dyn_div - 1) / dyn_div));
     __syncthreads();
     const u32 tile = s_tile;
+    if ((u64)tile * SCAN_TILE >= n && !(tile == 0 && total)) // past the length (tile 0 still writes the total)
+        return;
     const u64 base = (u64)tile * SCAN_TILE;
     const u64 i0 = base + (u64)threadIdx.x * SCAN_ITEMS;
     u32 v[SCAN_ITEMS];
@@ -224,14 +244,15 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(const u32 *__restrict__ i
         *total = s_prefix + aggregate;
 }
 
-void launch_scan(const u32 *in, u32 *out, u64 n, void *scratch, u32 *total, u32 *err, cudaStream_t st) {
+void launch_scan(const u32 *in, u32 *out, u64 n, void *scratch, u32 *total, u32 *err, cudaStream_t st,
+                 const u32 *n_dyn, u32 dyn_div, u32 dyn_mul) {
     if (n == 0)
         return;
     u64 tiles = scan_tiles(n);
     cudaMemsetAsync(scratch, 0, scan_scratch_bytes(n), st);
     u32 *counter = reinterpret_cast<u32 *>(scratch);
     u64 *status = reinterpret_cast<u64 *>(reinterpret_cast<char *>(scratch) + 256);
-    k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, out, n, counter, status, total, err);
+    k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, out, n, counter, status, total, err, n_dyn, dyn_div, dyn_mul);
 }
 
 // Withholds tile 0: the ticket counter starts at 1, so tiles 1..T wait on a tile that never
@@ -255,7 +276,7 @@ int selftest_lookback_timeout(int device, u32 n, u32 *err_out) {
         u32 one = 1;
         cudaMemcpy(scratch, &one, 4, cudaMemcpyHostToDevice); // ticket 0 is never handed out
         k_scan<<<(unsigned)tiles, SCAN_THREADS>>>((const u32 *)in, (u32 *)out, n, (u32 *)scratch,
-                                                  (u64 *)((char *)scratch + 256), nullptr, (u32 *)err);
+                                                  (u64 *)((char *)scratch + 256), nullptr, (u32 *)err, nullptr, 1u, 1u);
         if (cudaDeviceSynchronize() != cudaSuccess)
             rc = 3;
         cudaMemcpy(err_out, err, 4, cudaMemcpyDeviceToHost);
@@ -298,10 +319,18 @@ size_t radix_scratch_bytes(u64 n_max, u32 key_bits) {
     return 2 * hist * 4 + scan_scratch_bytes(hist) + 512;
 }
 
+// The launch covers the capacity's tiles; only the first T = ceil(n / RS_TILE) hold keys, and the
+// digit histograms are laid out [digit][T] for those alone, so the scan between the passes runs over
+// bins * T counters instead of bins * (capacity / RS_TILE).
+PHX_DI u32 radix_tiles(const u32 *n_dev) { return (u32)(((u64)*n_dev + RS_TILE - 1) / RS_TILE); }
+
 __global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const u32 *__restrict__ keys, const u32 *n_dev, u32 shift,
                                                           u32 bits, u32 *__restrict__ hist, u32 n_tiles) {
     extern __shared__ u32 sh[];
     const u32 bins = 1u << bits, mask = bins - 1u;
+    const u32 t_used = min(radix_tiles(n_dev), n_tiles);
+    if (blockIdx.x >= t_used)
+        return; // uniform for the block
     for (u32 d = threadIdx.x; d < bins; d += RS_THREADS)
         sh[d] = 0;
     __syncthreads();
@@ -317,7 +346,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const u32 *__restrict
     }
     __syncthreads();
     for (u32 d = threadIdx.x; d < bins; d += RS_THREADS)
-        hist[(u64)d * n_tiles + blockIdx.x] = sh[d];
+        hist[(u64)d * t_used + blockIdx.x] = sh[d];
 }
 
 __global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const u32 *__restrict__ keys_in,
@@ -327,17 +356,18 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const u32 *__restr
                                                              u32 n_tiles) {
     extern __shared__ u32 sh[];
     const u32 bins = 1u << bits, mask = bins - 1u;
+    const u32 t_used = min(radix_tiles(n_dev), n_tiles);
+    if (blockIdx.x >= t_used)
+        return; // uniform for the block
     u32 *cnt = sh;                     // [RS_WARPS][bins]
     u32 *gofs = sh + RS_WARPS * bins;  // [bins]
     for (u32 i = threadIdx.x; i < RS_WARPS * bins; i += RS_THREADS)
         cnt[i] = 0;
     for (u32 d = threadIdx.x; d < bins; d += RS_THREADS)
-        gofs[d] = hist_scanned[(u64)d * n_tiles + blockIdx.x];
+        gofs[d] = hist_scanned[(u64)d * t_used + blockIdx.x];
     __syncthreads();
     const u64 n = *n_dev;
     const u64 base = (u64)blockIdx.x * RS_TILE;
-    if (base >= n)
-        return; // uniform for the block
     const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const u32 lt_mask = (1u << lane) - 1u;
     u32 *wc = cnt + warp * bins;
@@ -402,7 +432,7 @@ void launch_radix_sort(const u32 *keys_in, u32 *keys_tmp0, u32 *keys_tmp1, u32 *
     for (u32 pass = 0; pass < p.passes; pass++) {
         u32 shift = pass * p.bits;
         k_radix_hist<<<(unsigned)tiles, RS_THREADS, smem_hist, st>>>(src_k, n_dev, shift, p.bits, hist, (u32)tiles);
-        launch_scan(hist, hist_scanned, hist_n, scan_scr, nullptr, err, st);
+        launch_scan(hist, hist_scanned, hist_n, scan_scr, nullptr, err, st, n_dev, (u32)RS_TILE, bins);
         bool last = pass + 1 == p.passes;
         k_radix_scatter<<<(unsigned)tiles, RS_THREADS, smem_scatter, st>>>(
             src_k, src_v, last ? nullptr : kt[pass & 1], vt[pass & 1], n_dev, shift, p.bits, hist_scanned, (u32)tiles);
@@ -421,26 +451,26 @@ __global__ void __launch_bounds__(256) k_sorted_records(const u32 *__restrict__ 
                                                        float4 *__restrict__ s_posdir, u32 *__restrict__ s_power,
                                                        float4 *__restrict__ s_dir, float4 *__restrict__ s_pow,
                                                        u64 n_max, u32 *err) {
-    u64 p = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p == 0 && *n_dev == 0)
+    const u64 n = min((u64)*n_dev, n_max);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && n == 0)
         atomicOr(err, ERR_NO_PHOTONS); // renderer.cpp:117-118 traps here
-    if (p >= *n_dev || p >= n_max)
-        return;
-    u32 i = perm[p];
-    float4 pos = ph_pos[i];
-    uint2 pd = ph_pd[i];
-    s_posdir[p] = make_float4(pos.x, pos.y, pos.z, __uint_as_float(pd.y));
-    s_power[p] = pd.x;
-    s_dir[p] = decode_oct(pd.y);
-    s_pow[p] = decode_rgbe(pd.x);
+    for (u64 p = (u64)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (u64)gridDim.x * blockDim.x) {
+        const u32 i = perm[p];
+        const float4 pos = ph_pos[i];
+        const uint2 pd = ph_pd[i];
+        s_posdir[p] = make_float4(pos.x, pos.y, pos.z, __uint_as_float(pd.y));
+        s_power[p] = pd.x;
+        s_dir[p] = decode_oct(pd.y);
+        s_pow[p] = decode_rgbe(pd.x);
+    }
 }
 
 void launch_sorted_records(const u32 *perm, const float4 *ph_pos, const uint2 *ph_pd, const u32 *n_dev, u64 n_max,
                            float4 *s_posdir, u32 *s_power, float4 *s_dir, float4 *s_pow, u32 *err, cudaStream_t st) {
     if (n_max == 0)
         return;
-    k_sorted_records<<<(unsigned)((n_max + 255) / 256), 256, 0, st>>>(perm, ph_pos, ph_pd, n_dev, s_posdir, s_power,
-                                                                    s_dir, s_pow, n_max, err);
+    k_sorted_records<<<stride_blocks(n_max, 256), 256, 0, st>>>(perm, ph_pos, ph_pd, n_dev, s_posdir, s_power, s_dir,
+                                                                s_pow, n_max, err);
 }
 
 // The decoded direction and power of records written from the host.
@@ -525,7 +555,7 @@ int scan_noalloc(const u32 *in, u32 *out, u32 n, u32 *total, cudaStream_t st, st
     u32 *counter = reinterpret_cast<u32 *>(scr);
     u32 *errw = counter + 1;
     u64 *status = reinterpret_cast<u64 *>(reinterpret_cast<char *>(scr) + 256);
-    k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, out, n, counter, status, total, errw);
+    k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, out, n, counter, status, total, errw, nullptr, 1u, 1u);
     if ((e = cudaGetLastError()) != cudaSuccess) {
         err = std::string("scan launch: ") + cudaGetErrorString(e);
         return 3;

@@ -95,7 +95,9 @@ void launch_hash(const LaunchCtx &lc, const GridBufs &g, const u32 *n_dev, u64 n
 // exclusive scan of n u32 (decoupled look-back).  total (optional) receives the sum.
 // scratch: ScanScratch sized by scan_scratch_words(n).
 size_t scan_scratch_bytes(u64 n);
-void launch_scan(const u32 *in, u32 *out, u64 n, void *scratch, u32 *total, u32 *err, cudaStream_t st);
+// n_dyn (optional): scan only min(n, dyn_mul * ceil(*n_dyn / dyn_div)) items, read on the device
+void launch_scan(const u32 *in, u32 *out, u64 n, void *scratch, u32 *total, u32 *err, cudaStream_t st,
+                 const u32 *n_dyn = nullptr, u32 dyn_div = 1, u32 dyn_mul = 1);
 // failure-detection self-test: scan with tile 0 withheld; returns 0 ok, 2 alloc, 3 CUDA error
 int selftest_lookback_timeout(int device, u32 n, u32 *err_out);
 // exclusive scan with its scratch in a static device array (no allocation); synchronous.
