@@ -571,7 +571,10 @@ void Engine::enq_trace_r(RoundSet &R, cudaStream_t s) {
         transmissive = transmissive || sl.desc.any_transmissive != 0;
         presample = presample || sl.desc.light_draws == LIGHT_DRAWS_VARY;
     }
-    launch_shadow(l, o, transmissive ? SHADOW_GENERAL : SHADOW_OPAQUE, presample, s);
+    // every sample of a hit point is one ray when the only light is a point, spot or directional one
+    const bool per_pixel = sc.size() == 1 && shard.world == 1 && sc[0].lights.size() == 1 &&
+                           sc[0].lights[0].kind != PHX_LIGHT_TEXTURED;
+    launch_shadow(l, o, transmissive ? SHADOW_GENERAL : SHADOW_OPAQUE, presample, per_pixel, sc[0].desc.n_pixels, s);
     launch_nee_resolve(l, o, s);
     if (spec)
         launch_spec_resolve(l, o, s);

@@ -588,27 +588,33 @@ __global__ void __launch_bounds__(128, PHX_TRACE_MINB) k_trace_persistent(Launch
 // ---- shadow wavefront ---------------------------------------------------------------------------
 // One thread per recorded NEE sample; the ds samples of a pixel are consecutive threads, so a warp
 // traces shadow rays from one or two hit points toward the same light: coherent traversal.
-template <int KIND> PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 first_block);
+template <int KIND, bool PER_PIXEL> PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 first_block);
 
 // Blocks [0, nee_blocks): one diffuse sample slot per thread.  Blocks from nee_blocks on (only when
 // the specular NEE is deferred): the specular sample slots, grid-stride; being last in the grid
 // they start as the diffuse blocks drain and fill the launch's tail.  KIND: the scenes' kind
 // (SHADOW_*), chosen on the host.
-template <int KIND>
+// per_pixel (a single scene whose only light is a point, spot or directional light): choosing that
+// light is a sample's only random draw, so all ds samples of a hit point are the same ray with the
+// same weight; one thread per pixel traces sample 0 and writes its contribution to the pixel's ds
+// slots, which k_nee_resolve then sums as before (the same values in the same order).
+template <int KIND, bool PER_PIXEL>
 __global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow(LaunchCtx lc, TraceOut out, u32 nee_blocks) {
+    constexpr bool per_pixel = PER_PIXEL;
     if (blockIdx.x >= nee_blocks) {
-        shadow_spec_slots<KIND>(lc, out, nee_blocks);
+        shadow_spec_slots<KIND, PER_PIXEL>(lc, out, nee_blocks);
         return;
     }
-    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= lc.total_nee)
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (per_pixel ? lc.scenes[0].n_pixels : lc.total_nee))
         return;
-    const u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.nee_bases, lc.n_scenes, g);
+    const u32 s = per_pixel || lc.n_scenes == 1 ? 0 : find_scene(lc.nee_bases, lc.n_scenes, t);
     const SceneDesc &sc = lc.scenes[s];
     if (!sc.active)
         return;
     const u32 ds = sc.direct_samples;
-    const u32 pixel = (g - sc.nee_base) / ds;
+    const u32 pixel = per_pixel ? t : (t - sc.nee_base) / ds;
+    const u32 g = per_pixel ? sc.nee_base + pixel * ds : t; // this thread's (first) sample slot
     const u32 gpix = sc.pixel_base + pixel;
     if (out.emission[gpix].w != 1.0f)
         return; // no diffuse hit point: the slot was not used this round
@@ -639,19 +645,29 @@ __global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow(LaunchCtx lc, T
         u32 ovf = 0;
         contrib = w * shadow_transmittance<KIND>(sc, pos, dir, dist, &ovf); // frag.radiance * (base / PI) * trans
         if (ovf)
-            atomicAdd(lc.overflow, ovf);
+            atomicAdd(lc.overflow, per_pixel ? ovf * ds : ovf);
     }
-    out.nee_val[g] = contrib;
+    if (per_pixel) {
+        for (u32 i = 0; i < ds; i++)
+            out.nee_val[g + i] = contrib;
+    } else {
+        out.nee_val[g] = contrib;
+    }
 }
 
 // Deferred specular NEE samples: one thread per claimed sample slot.  An event's samples are
 // consecutive, so a warp traces rays from one or two hit points toward the lights together.  The
 // contribution is the traced form's: weight * transmittance, zero for a sample without a ray.
-template <int KIND> PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 first_block) {
+// per_pixel (see k_shadow): an event's ds samples, ds consecutive slots from a multiple of ds, are
+// one ray with one weight: one thread per event traces its first slot and fills all ds.
+template <int KIND, bool PER_PIXEL>
+PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 first_block) {
     const u32 n = min(*out.spec_next, out.spec_cap);
     const u32 stride = (gridDim.x - first_block) * blockDim.x;
+    const u32 step = PER_PIXEL ? lc.scenes[0].direct_samples : 1u;
     u32 ovf = 0;
-    for (u32 g = (blockIdx.x - first_block) * blockDim.x + threadIdx.x; g < n; g += stride) {
+    for (u32 e = (blockIdx.x - first_block) * blockDim.x + threadIdx.x; (u64)e * step < n; e += stride) {
+        const u32 g = e * step;
         const u32 gpix = out.spec_pix[g];
         const SceneDesc &sc = lc.scenes[lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gpix)];
         const float4 hdr = out.spec_ray[g];
@@ -684,9 +700,13 @@ template <int KIND> PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const Tra
             }
         }
         float4 contrib = zero4();
-        if (!(dist < 0.0f))
-            contrib = w * shadow_transmittance<KIND>(sc, org, dir, dist, &ovf);
-        out.spec_val[g] = contrib;
+        if (!(dist < 0.0f)) {
+            u32 o_ = 0;
+            contrib = w * shadow_transmittance<KIND>(sc, org, dir, dist, &o_);
+            ovf += o_ * step;
+        }
+        for (u32 i = 0; i < step; i++)
+            out.spec_val[g + i] = contrib;
     }
     if (ovf)
         atomicAdd(lc.overflow, ovf);
@@ -775,17 +795,24 @@ __global__ void __launch_bounds__(128) k_nee_sample(LaunchCtx lc, TraceOut out) 
     record_nee(sc, &rng, out.pos[gpix], out.stash_sn[gpix], out.base_color[gpix], out, slot);
 }
 
-void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int kind, bool presample, cudaStream_t st) {
+void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int kind, bool presample, bool per_pixel,
+                   u32 n_pixels, cudaStream_t st) {
     if (!lc.nee_defer || lc.total_nee == 0)
         return;
     if (presample && lc.pix_hi > lc.pix_lo)
         k_nee_sample<<<(lc.pix_hi - lc.pix_lo + 127) / 128, 128, 0, st>>>(lc, out);
-    const u32 nee_blocks = (lc.total_nee + 127) / 128;
+    per_pixel = per_pixel && !presample && lc.n_scenes == 1;
+    const u32 nee_blocks = ((per_pixel ? n_pixels : lc.total_nee) + 127) / 128;
     const u32 spec_blocks = out.spec_ray && out.spec_cap ? (u32)g_sm_count * 8u : 0u;
-    if (kind == SHADOW_OPAQUE)
-        k_shadow<SHADOW_OPAQUE><<<nee_blocks + spec_blocks, 128, 0, st>>>(lc, out, nee_blocks);
+    const u32 grid = nee_blocks + spec_blocks;
+    if (kind == SHADOW_OPAQUE && per_pixel)
+        k_shadow<SHADOW_OPAQUE, true><<<grid, 128, 0, st>>>(lc, out, nee_blocks);
+    else if (kind == SHADOW_OPAQUE)
+        k_shadow<SHADOW_OPAQUE, false><<<grid, 128, 0, st>>>(lc, out, nee_blocks);
+    else if (per_pixel)
+        k_shadow<SHADOW_GENERAL, true><<<grid, 128, 0, st>>>(lc, out, nee_blocks);
     else
-        k_shadow<SHADOW_GENERAL><<<nee_blocks + spec_blocks, 128, 0, st>>>(lc, out, nee_blocks);
+        k_shadow<SHADOW_GENERAL, false><<<grid, 128, 0, st>>>(lc, out, nee_blocks);
 }
 
 void launch_nee_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st) {

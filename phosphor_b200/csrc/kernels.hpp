@@ -63,7 +63,9 @@ void launch_trace(const LaunchCtx &lc, const TraceOut &out, int block, int persi
 // each pixel's samples in sample order into hp_direct.
 // kind: SHADOW_OPAQUE when no scene has a transmissive material, else SHADOW_GENERAL.  presample:
 // some scene's light samples take varying RNG draws, so k_nee_sample draws its samples first.
-void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int kind, bool presample, cudaStream_t st);
+// per_pixel: a single scene whose only light is not an area light (one shadow ray per hit point)
+void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int kind, bool presample, bool per_pixel,
+                   u32 n_pixels, cudaStream_t st);
 void launch_nee_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st);
 // Deferred specular NEE: complete each listed pixel's emission once k_shadow has traced the
 // claimed sample slots.
