@@ -48,8 +48,7 @@ CONFIGS = {
                    desc="procedural atrium, 262,898 triangles, 1920x1080, 2^22 photons/iter, depth 16"),
 }
 METRIC = "Mphotons/s"
-# dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu capture of the full-size
-# workload (profiles/dram_traffic_caustic_1024.md)
+# dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu capture
 # (a stage's kernels summed; the shadow stage: k_shadow, k_nee_resolve, k_spec_resolve — k_nee_sample
 # does not run for scenes whose light samples all take the same RNG draws)
 NCU_TRAFFIC = {"caustic": {"trace": 939_781_376, "shadow": 991_296_512, "emit": 465_910_784,
@@ -135,9 +134,8 @@ def cpu_oracle_sample(cfg: dict, threads: int, min_seconds: float = 10.0, max_ro
     """The reference algorithm (oracle port, fp32) on the host cores, on the workload itself: one
     untimed round, then whole rounds until `min_seconds` have passed (at most `max_rounds`)."""
     import oracle as O
-    import phosphor_b200 as P
     args = make_args(cfg, 1)
-    scene = P.SceneData.generate(cfg["kind"], seed=1, width=args.width, height=args.height, detail=cfg["detail"])
+    scene = O.GeneratedScene(cfg["kind"], seed=1, width=args.width, height=args.height, detail=cfg["detail"])
     orc = O.Oracle(scene)
     state = orc.render(args.params(), 1, prec=0, threads=threads)  # warm-up round
     dt, rounds, stage = 0.0, 0, [0.0] * 4
@@ -161,9 +159,9 @@ def run_reference(a, cfg: dict) -> dict:
     # the run longer than a few minutes; then 1/scale of the resolution and 1/scale^2 of the photons
     scale = 1 if a.steps + a.warmup <= 40 else 2 if a.steps + a.warmup <= 160 else 4
     import oracle as O
-    import phosphor_b200 as P
     args = make_args(cfg, scale)
-    scene = P.SceneData.generate(cfg["kind"], seed=1, width=args.width, height=args.height, detail=cfg["detail"])
+    # the scene comes from the oracle library's copy of the generators: this arm maps no CUDA library
+    scene = O.GeneratedScene(cfg["kind"], seed=1, width=args.width, height=args.height, detail=cfg["detail"])
     orc = O.Oracle(scene)
     state = None
     for _ in range(a.warmup):

@@ -425,7 +425,9 @@ PHX_API int phx_selftest_lookback_timeout(int device, uint32_t n, uint32_t *err_
  *   - stream: a cudaStream_t (0 = legacy default stream).  The call enqueues its work there and
  *     then waits for that stream to finish, so the result is ready on return.
  *   - the first call on each device looks up the scratch array's address (cudaGetSymbolAddress)
- *     with that device current; make it before any stream capture on that device.
+ *     with that device current; make it before any stream capture on that device.  The address
+ *     is kept per CUDA context: the first call after cudaDeviceReset, or under another driver-API
+ *     context, looks it up again (so it too should precede any capture).
  *   - calls share the one scratch array per device: two calls whose scans overlap on the GPU
  *     (different streams, or different host threads) race on it and give wrong results.
  * Returns PHX_E_TIMEOUT if a bounded look-back wait gave up (results then invalid). */

@@ -29,6 +29,8 @@ def load() -> C.CDLL:
     lib = C.CDLL(str(LIB_PATH))
     vp = C.c_void_p
     sig = {
+        "orc_scene_generate": (C.c_int, [vp, vp, vp]),
+        "orc_scene_free": (None, [vp]),
         "orc_bvh_build": (C.c_int, [vp, C.c_uint32, vp, vp]),
         "orc_hash_info": (C.c_int, [vp, C.c_uint32, vp]),
         "orc_create": (vp, [vp]),
@@ -75,8 +77,32 @@ def default_threads() -> int:
     return max(1, os.cpu_count() or 1)
 
 
+class GeneratedScene:
+    """A procedural scene built by the oracle library's copy of the scene generators, in the same
+    phx_scene layout as phosphor_b200.SceneData.generate (same generator source, same seeded output).
+    CPU-only callers use it so that nothing maps the CUDA library."""
+
+    def __init__(self, kind: int, seed: int = 1, width: int = 512, height: int = 512, detail: int = 0):
+        from phosphor_b200 import _capi as A  # ctypes declarations only; loads no library
+        self.lib = load()
+        spec = A.SceneSpec(kind=kind, seed=seed, width=width, height=height, detail=detail)
+        self.scene = A.Scene()
+        self._h = C.c_void_p()
+        _chk(self.lib.orc_scene_generate(C.byref(spec), C.byref(self.scene), C.byref(self._h)))
+
+    @property
+    def n_triangles(self) -> int:
+        return self.scene.n_triangles
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self.lib.orc_scene_free(self._h)
+            self._h = None
+
+
 class Oracle:
-    """Reference restatement bound to one scene (phx_scene from phosphor_b200.SceneData)."""
+    """Reference restatement bound to one scene (phx_scene from phosphor_b200.SceneData or
+    GeneratedScene)."""
 
     def __init__(self, scene):
         self.lib = load()

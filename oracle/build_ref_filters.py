@@ -10,13 +10,14 @@ way an NDRange of (width, height) work items would.  gcc compiles it without con
 (-ffp-contract=off), so every float operation is the one written.  The output goes to
 oracle/_ref/ only (git-ignored); nothing from the reference enters the repository.
 
-    python oracle/build_ref_filters.py [path/to/reference]
+    python oracle/build_ref_filters.py path/to/reference     (or PHX_REFERENCE_DIR=path/to/reference)
 
 tests/golden/make_denoise_golden.py runs the result to make the committed fixtures.
 """
 from __future__ import annotations
 
 import ast
+import os
 import subprocess
 import sys
 from pathlib import Path
@@ -62,14 +63,23 @@ def kernel_source(reference: Path) -> str:
     raise RuntimeError("_KERNEL_SOURCE not found in denoise/filters_gpu.py")
 
 
-DEFAULT_REFERENCE = Path("/root/reference")
+def reference_dir(arg: str | os.PathLike | None = None) -> Path | None:
+    """The reference checkout: the given path, else $PHX_REFERENCE_DIR, else None (no default)."""
+    if arg:
+        return Path(arg)
+    env = os.environ.get("PHX_REFERENCE_DIR")
+    return Path(env) if env else None
 
 
-def reference_present(reference: Path = DEFAULT_REFERENCE) -> bool:
-    return (reference / "denoise" / "filters_gpu.py").is_file()
+def reference_present(reference: Path | None = None) -> bool:
+    reference = reference_dir(reference)
+    return reference is not None and (reference / "denoise" / "filters_gpu.py").is_file()
 
 
-def build(reference: Path = DEFAULT_REFERENCE, verbose: bool = False) -> Path:
+def build(reference: Path | None = None, verbose: bool = False) -> Path:
+    reference = reference_dir(reference)
+    if reference is None:
+        raise RuntimeError("no reference checkout given (argument or PHX_REFERENCE_DIR)")
     src = PRELUDE + kernel_source(reference) + DRIVER
     OUT.parent.mkdir(parents=True, exist_ok=True)
     cmd = ["gcc", "-O2", "-std=c99", "-fPIC", "-shared", "-ffp-contract=off", "-x", "c", "-o", str(OUT), "-"]
@@ -82,4 +92,4 @@ def build(reference: Path = DEFAULT_REFERENCE, verbose: bool = False) -> Path:
 
 
 if __name__ == "__main__":
-    build(Path(sys.argv[1]) if len(sys.argv) > 1 else DEFAULT_REFERENCE, verbose=True)
+    build(sys.argv[1] if len(sys.argv) > 1 else None, verbose=True)

@@ -4,6 +4,10 @@
 #include "phx_frozen.hpp"
 #include "phx_oracle.hpp"
 
+// the procedural scene generators (phosphor_b200/csrc/scenes.cpp, compiled into this library too):
+// the seeded synthetic inputs, so that a CPU-only run of the oracle never loads the CUDA library
+#include "../phosphor_b200/csrc/host.hpp"
+
 #include <atomic>
 #include <chrono>
 #include <functional>
@@ -373,6 +377,26 @@ void image_impl(const void *flux, const void *radiance, u32 n, float exposure, i
 } // namespace
 
 extern "C" {
+
+__attribute__((visibility("default"))) int orc_scene_generate(const phx_scene_spec *spec, phx_scene *out,
+                                                             void **handle) {
+    if (!spec || !out || !handle)
+        return PHX_E_INVALID;
+    auto *st = new phx::SceneStore();
+    std::string err;
+    int r = phx::scene_generate(*spec, *st, err);
+    if (r) {
+        delete st;
+        return r;
+    }
+    st->view(out);
+    *handle = st;
+    return PHX_OK;
+}
+
+__attribute__((visibility("default"))) void orc_scene_free(void *handle) {
+    delete reinterpret_cast<phx::SceneStore *>(handle);
+}
 
 __attribute__((visibility("default"))) int orc_bvh_build(const phx_triangle *tris, uint32_t n, phx_bvh_node *out,
                                                         uint32_t *depth) {

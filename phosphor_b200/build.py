@@ -102,14 +102,16 @@ def build_cli(force: bool = False, verbose: bool = False) -> Path:
 
 def build_oracle(force: bool = False, verbose: bool = False) -> Path:
     """Compiles the CPU oracle (test infrastructure only; see oracle/phx_oracle.hpp)."""
-    srcs = [ORACLE_DIR / "oracle_capi.cpp"]
+    # the scene generators are host-only C++ shared with the library (synthetic inputs, not the
+    # checked algorithm), so CPU-only callers of the oracle never map libphx.so
+    srcs = [ORACLE_DIR / "oracle_capi.cpp", CSRC / "scenes.cpp"]
     deps = srcs + [ORACLE_DIR / "phx_oracle.hpp", ORACLE_DIR / "phx_frozen.hpp", INCLUDE / "phx.h",
-                   INCLUDE / "phx_math.h"]
+                   INCLUDE / "phx_math.h", CSRC / "host.hpp"]
     if not force and ORACLE_LIB.exists() and ORACLE_LIB.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
         return ORACLE_LIB
     tmp = ORACLE_LIB.with_suffix(".so.tmp")
     cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fvisibility=hidden", "-ffp-contract=off",
-           "-o", str(tmp), *map(str, srcs), "-lpthread"]
+           "-I", str(INCLUDE), "-o", str(tmp), *map(str, srcs), "-lpthread"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"oracle build failed\n{res.stdout}\n{res.stderr}")

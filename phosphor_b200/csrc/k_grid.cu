@@ -507,11 +507,37 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = 256 + 8 * (size_t)NOALLOC_SCAN_MAX_TILE
 static __device__ __align__(256) unsigned char g_noalloc_scan_scratch[NOALLOC_SCRATCH_BYTES];
 
 // Host-side address of g_noalloc_scan_scratch on each device.  The array's name in host code is a
-// stand-in, not a device address, so the address is looked up once per device (with that device
-// current) through cudaGetSymbolAddress and passed to the kernel.  That set-up happens in the first
-// call on each device, which should therefore come before any stream capture on it.
+// stand-in, not a device address, so the address is looked up (with the device current) through
+// cudaGetSymbolAddress and passed to the kernel.  The look-up is the set-up of the first call on each
+// device, which should therefore come before any stream capture on it.  The cached address belongs
+// to the CUDA context it was looked up in: after cudaDeviceReset, or under another driver-API
+// context on the same device, the module is loaded anew and the address changes, so each entry
+// records its context and a call made under a different one repeats the set-up.
+using CtxGetCurrentFn = int (*)(void **);
 static std::mutex g_noalloc_mu;
-static void *g_noalloc_ptr[128] = {};
+struct NoallocScratch {
+    void *ctx = nullptr;
+    void *ptr = nullptr;
+};
+static NoallocScratch g_noalloc[128];
+
+static void *current_context() {
+    static CtxGetCurrentFn fn = []() -> CtxGetCurrentFn {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess) {
+            cudaGetLastError();
+            f = nullptr;
+        } else if (q != cudaDriverEntryPointSuccess) {
+            f = nullptr;
+        }
+        return reinterpret_cast<CtxGetCurrentFn>(f);
+    }();
+    void *ctx = nullptr;
+    if (!fn || fn(&ctx) != 0)
+        return nullptr;
+    return ctx;
+}
 
 int scan_noalloc(const u32 *in, u32 *out, u32 n, u32 *total, cudaStream_t st, std::string &err) {
     if (n > NOALLOC_SCAN_MAX_N) {
@@ -528,20 +554,25 @@ int scan_noalloc(const u32 *in, u32 *out, u32 n, u32 *total, cudaStream_t st, st
     void *scr;
     {
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
+        void *ctx = current_context();
+        NoallocScratch &c = g_noalloc[dev];
+        if (!c.ptr || !ctx || c.ctx != ctx) {
             void *p = nullptr;
-            e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
+            e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch); // also makes the primary context current
             if (e != cudaSuccess || !p) {
                 err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
                 return 3;
             }
-            g_noalloc_ptr[dev] = p;
+            c.ptr = p;
+            c.ctx = current_context();
         }
-        scr = g_noalloc_ptr[dev];
+        scr = c.ptr;
     }
     if (n == 0) {
-        if (total && (e = cudaMemsetAsync(total, 0, 4, st)) != cudaSuccess) {
-            err = std::string("cudaMemsetAsync: ") + cudaGetErrorString(e);
+        // like every other size, the call returns with the result written
+        if (total && ((e = cudaMemsetAsync(total, 0, 4, st)) != cudaSuccess ||
+                      (e = cudaStreamSynchronize(st)) != cudaSuccess)) {
+            err = std::string("scan (n = 0): ") + cudaGetErrorString(e);
             return 3;
         }
         return 0;

@@ -51,4 +51,8 @@ def main(reference: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    from oracle.build_ref_filters import reference_dir
+    ref = reference_dir(sys.argv[1] if len(sys.argv) > 1 else None)
+    if ref is None:
+        sys.exit("usage: make_denoise_golden.py path/to/reference   (or set PHX_REFERENCE_DIR)")
+    main(ref)
