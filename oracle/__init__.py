@@ -3,8 +3,9 @@
 The oracle is a statement-by-statement C++ restatement of the reference SPPM kernels (see
 oracle/phx_oracle.hpp for the file:line map and the fixed semantics).  Only tests/,
 __graft_entry__.smoke() and bench.py's CPU-baseline leg use it, as the checker; the library never
-calls it.  PARITY UNPINNED BY THE REFERENCE: the reference ships no golden vectors and cannot run
-here; the restatement is pinned by hand-derived known answers in tests/golden/.
+calls it.  Pinned to the reference itself: tests/test_ref_pin.py compares it stage by stage with
+the reference's own kernels and host code compiled for the CPU (oracle/build_ref_sppm.py,
+fixtures in tests/golden/ref_sppm_golden.npz).
 """
 from __future__ import annotations
 
@@ -31,6 +32,8 @@ def load() -> C.CDLL:
     sig = {
         "orc_scene_generate": (C.c_int, [vp, vp, vp]),
         "orc_scene_free": (None, [vp]),
+        "orc_camera_make": (None, [vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, vp]),
+        "orc_lum_pref_sum": (None, [vp, C.c_uint32, vp]),
         "orc_bvh_build": (C.c_int, [vp, C.c_uint32, vp, vp]),
         "orc_hash_info": (C.c_int, [vp, C.c_uint32, vp]),
         "orc_create": (vp, [vp]),
@@ -296,3 +299,17 @@ def get_hash(p4, hash_data: bytes):
 def math(fn: str, x: float, y: float = 0.0) -> float:
     code = {"sin": 0, "cos": 1, "exp": 2, "log": 3, "pow": 4, "acos": 5, "atan2": 6}[fn]
     return float(load().orc_math(code, x, y))
+
+
+def camera_make(pos, at, up, hfov: float, aspect: float, defocus: float = 0.0, focus: float = 1.0) -> bytes:
+    """The scene generators' camera (Camera + focus + to_params) as 112 bytes of CameraParams."""
+    f = [np.ascontiguousarray(v, np.float32) for v in (pos, at, up)]
+    out = (C.c_uint8 * 112)()
+    load().orc_camera_make(_p(f[0]), _p(f[1]), _p(f[2]), hfov, aspect, defocus, focus, out)
+    return bytes(out)
+
+
+def lum_pref_sum(lights_ptr, n: int) -> np.ndarray:
+    out = np.empty(n, np.float32)
+    load().orc_lum_pref_sum(lights_ptr, n, _p(out))
+    return out

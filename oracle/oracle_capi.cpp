@@ -1,6 +1,6 @@
 // oracle_capi.cpp — TEST INFRASTRUCTURE ONLY: extern "C" entry points of the CPU oracle
 // (liboracle.so), called through ctypes by tests/ and by bench.py's CPU-baseline leg.
-// PARITY UNPINNED BY THE REFERENCE (see phx_oracle.hpp).
+// Pinned to the reference's own code compiled for the CPU (see phx_oracle.hpp).
 #include "phx_frozen.hpp"
 #include "phx_oracle.hpp"
 
@@ -396,6 +396,18 @@ __attribute__((visibility("default"))) int orc_scene_generate(const phx_scene_sp
 
 __attribute__((visibility("default"))) void orc_scene_free(void *handle) {
     delete reinterpret_cast<phx::SceneStore *>(handle);
+}
+
+// the generators' camera (Camera + focus + to_params) and light luminance prefix sum, for checks
+// against the reference's own camera.cpp and scene_data.cpp
+__attribute__((visibility("default"))) void orc_camera_make(const float *pos, const float *at, const float *up,
+                                                           float hfov, float aspect, float defocus, float focus,
+                                                           phx_camera_params *out) {
+    phx::camera_make(pos, at, up, hfov, aspect, defocus, focus, out);
+}
+
+__attribute__((visibility("default"))) void orc_lum_pref_sum(const phx_light *lights, uint32_t n, float *out) {
+    phx::lum_pref_sum(lights, n, out);
 }
 
 __attribute__((visibility("default"))) int orc_bvh_build(const phx_triangle *tris, uint32_t n, phx_bvh_node *out,

@@ -5,10 +5,12 @@
 // sequentially in a canonical order.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
 // baseline use it; the library never links or calls it.
 //
-// PARITY UNPINNED BY THE REFERENCE: the reference (alfazet/phosphor) ships no golden vectors,
-// known-answer tests or fixtures for this path, and it cannot be executed here (its kernels need
-// an OpenCL runtime, absent both here and on the GPU box; its host needs network-fetched deps).
-// The restatement is checked instead against hand-derived known answers (tests/golden/).
+// PINNED TO THE REFERENCE ITSELF: the reference (alfazet/phosphor) ships no golden vectors and
+// has no OpenCL runtime to run on here, so oracle/build_ref_sppm.py compiles its own kernels
+// (kernels/*.cl with include/{common,device}/*.h, vector literals and one swizzle rewritten) and
+// its host BVH builder, camera, light constructors and image formation for the CPU, with the
+// builtins fixed as below.  tests/test_ref_pin.py checks this restatement against that build's
+// outputs (tests/golden/ref_sppm_golden.npz): every stage bit for bit on eight scenes.
 //
 // Fixed choices where OpenCL leaves freedom (the same choices the device code makes):
 //  * IEEE-754 binary32 arithmetic with no contraction (build with -ffp-contract=off);
