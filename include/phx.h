@@ -324,7 +324,9 @@ typedef struct phx_tuning {
                                    and photon passes on branches of their own (they depend only on
                                    the round seed) and the gathers in round order, so rounds overlap;
                                    k - 1 extra sets of per-round buffers (1..8, 1 = off) */
-    uint32_t reserved[2];
+    uint32_t gather_coop;       /* 1 = a warp stages each cell's photon records in shared memory and its
+                                   lanes that need the cell walk them; 0 = one thread per pixel */
+    uint32_t reserved[1];
 } phx_tuning;
 PHX_API int phx_get_tuning(void *ctx, phx_tuning *out);
 PHX_API int phx_set_tuning(void *ctx, const phx_tuning *in);

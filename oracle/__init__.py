@@ -58,6 +58,7 @@ def load() -> C.CDLL:
         "orc_get_hash": (None, [vp, C.c_uint32, vp, vp]),
         "orc_math": (C.c_float, [C.c_int, C.c_float, C.c_float]),
         "orc_frozen_render": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, vp, C.c_uint32, C.c_int, vp, vp, vp]),
+        "orc_frozen_grad": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, vp, C.c_uint32, vp, C.c_int, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -189,6 +190,25 @@ class Oracle:
         _chk(self.lib.orc_frozen_render(self.h, C.addressof(params), rounds, _p(mats), len(mats), _p(lts), len(lts),
                                         threads or default_threads(), _p(img), _p(flux), _p(rad)))
         return img, flux, rad
+
+
+def _frozen_grad(self, params, rounds: int, materials: np.ndarray, lights: np.ndarray, g_img: np.ndarray,
+                 threads: int | None = None):
+    """The analytic FP64 gradient of L(θ) = Σ g·F(θ) (forward-mode dual numbers through the
+    frozen-path estimator) at θ = (materials, lights): (gradient laid out like
+    phosphor_b200.adjoint.ParamTable, L)."""
+    mats = np.ascontiguousarray(materials)
+    lts = np.ascontiguousarray(lights)
+    g = np.ascontiguousarray(g_img, dtype=np.float64).reshape(-1)
+    assert g.size == 3 * params.width * params.height
+    grad = np.zeros(4 * len(mats) + 3 * len(lts), np.float64)
+    loss = C.c_double()
+    _chk(self.lib.orc_frozen_grad(self.h, C.addressof(params), rounds, _p(mats), len(mats), _p(lts), len(lts), _p(g),
+                                  threads or default_threads(), _p(grad), C.byref(loss)))
+    return grad, loss.value
+
+
+Oracle.frozen_grad = _frozen_grad
 
 
 def bvh_build(tris_ptr, n: int):

@@ -268,39 +268,39 @@ int render_impl(OrcCtx *o, const phx_params *p, u32 rounds, int threads, void *f
 }
 
 // The frozen-path estimator F(θ') (phx_frozen.hpp) over `rounds` rounds from a fresh state:
-// linear image (radiance/R + flux/(π r² N)) in double into img1 (npx x 3); the θ0 float state
-// (bit-identical to render_impl<float>) into flux0/radiance0 when given.
-int frozen_render_impl(OrcCtx *o, const phx_params *p, u32 rounds, const frozen::Primed &pr, int threads,
-                       double *img1, float *flux0, float *radiance0) {
-    using frozen::D4;
+// linear image (radiance/R + flux/(π r² N)) in the scalar type S into img1 (npx x 3); the θ0 float
+// state (bit-identical to render_impl<float>) into flux0/radiance0 when given.
+template <class S>
+int frozen_render_impl(OrcCtx *o, const phx_params *p, u32 rounds, const frozen::Primed<S> &pr, int threads,
+                       S *img1, float *flux0, float *radiance0) {
     u32 npx = p->width * p->height;
     u32 buckets = p->grid_res * p->grid_res * p->grid_res + 1;
     u32 maxb = p->max_photon_bounces, ne = p->photons_per_round;
     phx_photon_hash_data hd = hash_info(o->bvh[0], p->grid_res);
     std::vector<HitPoint<float>> hp(npx);
-    std::vector<frozen::HitPrimed> hp1(npx);
+    std::vector<frozen::HitPrimed<S>> hp1(npx);
     std::vector<StoredPhoton<float>> slots((size_t)ne * maxb);
-    std::vector<D4> slot_pow1((size_t)ne * maxb);
+    std::vector<V4<S>> slot_pow1((size_t)ne * maxb);
     std::vector<u32> cnt(ne);
     std::vector<V4<float>> flux(npx, zero4<float>()), radiance(npx, zero4<float>());
     std::vector<float> weight(npx, 0.0f);
-    std::vector<D4> flux1(npx, zero4<double>()), rad1(npx, zero4<double>());
+    std::vector<V4<S>> flux1(npx, zero4<S>()), rad1(npx, zero4<S>());
     std::vector<u32> counts(buckets), start(buckets), end(buckets);
     Rng rng = pcg_seed(p->seed);
     for (u32 round = 0; round < rounds; round++) {
         u32 seed = random_u32(&rng);
         parallel_for(npx, threads, [&](u32 b, u32 e) {
             for (u32 i = b; i < e; i++)
-                hp[i] = frozen::trace_pixel(o->sc, pr, p->width, p->height, seed, p->direct_samples, i, &hp1[i]);
+                hp[i] = frozen::trace_pixel<S>(o->sc, pr, p->width, p->height, seed, p->direct_samples, i, &hp1[i]);
         });
         parallel_for(ne, threads, [&](u32 b, u32 e) {
             for (u32 i = b; i < e; i++)
-                cnt[i] = frozen::emit_photon(o->sc, pr, i, maxb, seed, &slots[(size_t)i * maxb],
-                                             &slot_pow1[(size_t)i * maxb]);
+                cnt[i] = frozen::emit_photon<S>(o->sc, pr, i, maxb, seed, &slots[(size_t)i * maxb],
+                                                &slot_pow1[(size_t)i * maxb]);
         });
         std::vector<float> pos;
         std::vector<u32> power, dir;
-        std::vector<D4> pow1;
+        std::vector<V4<S>> pow1;
         for (u32 i = 0; i < ne; i++) // canonical order: path, then bounce
             for (u32 j = 0; j < cnt[i]; j++) {
                 const StoredPhoton<float> &s = slots[(size_t)i * maxb + j];
@@ -318,24 +318,24 @@ int frozen_render_impl(OrcCtx *o, const phx_params *p, u32 rounds, const frozen:
         reference_scan(counts.data(), buckets, start.data());
         scatter_impl<float>(pos.data(), power.data(), dir.data(), keys.data(), n, start.data(), buckets, spos.data(),
                             spower.data(), sdir.data(), end.data(), perm.data());
-        std::vector<D4> spow1(n);
+        std::vector<V4<S>> spow1(n);
         for (u32 k = 0; k < n; k++)
             spow1[k] = pow1[perm[k]];
         const V4<float> *sp = (const V4<float> *)spos.data();
         parallel_for(npx, threads, [&](u32 b, u32 e) {
             for (u32 i = b; i < e; i++)
-                frozen::gather_pixel(hp[i], hp1[i], hd, start.data(), end.data(), sp, spower.data(), sdir.data(),
-                                     spow1.data(), p->sppm_alpha, &flux[i], &weight[i], &radiance[i], &flux1[i],
-                                     &rad1[i]);
+                frozen::gather_pixel<S>(hp[i], hp1[i], hd, start.data(), end.data(), sp, spower.data(), sdir.data(),
+                                        spow1.data(), p->sppm_alpha, &flux[i], &weight[i], &radiance[i], &flux1[i],
+                                        &rad1[i]);
         });
     }
     const double n_total = (double)p->photons_per_round * rounds;
     for (u32 i = 0; i < npx; i++) {
         const double area = (double)PI_F * flux[i].w;
         const double per = area > 0.0 ? 1.0 / (area * n_total) : 0.0;
-        img1[3 * (size_t)i + 0] = rad1[i].x / rounds + flux1[i].x * per;
-        img1[3 * (size_t)i + 1] = rad1[i].y / rounds + flux1[i].y * per;
-        img1[3 * (size_t)i + 2] = rad1[i].z / rounds + flux1[i].z * per;
+        img1[3 * (size_t)i + 0] = rad1[i].x / S((double)rounds) + flux1[i].x * S(per);
+        img1[3 * (size_t)i + 1] = rad1[i].y / S((double)rounds) + flux1[i].y * S(per);
+        img1[3 * (size_t)i + 2] = rad1[i].z / S((double)rounds) + flux1[i].z * S(per);
         if (flux0)
             store4<float>(flux0, i, flux[i]);
         if (radiance0)
@@ -540,8 +540,65 @@ __attribute__((visibility("default"))) int orc_frozen_render(void *o, const phx_
     if (!c || !p || !img1 || rounds == 0 || n_mats != c->n_materials || n_lights != c->sc.n_lights ||
         (n_mats && !mats1) || (n_lights && !lights1))
         return PHX_E_INVALID;
-    frozen::Primed pr{mats1, lights1};
-    return frozen_render_impl(c, p, rounds, pr, threads, img1, flux4, radiance4);
+    frozen::PrimedTables t(mats1, n_mats, lights1, n_lights);
+    frozen::Primed<double> pr{mats1, lights1, t.base.data(), t.rough.data(), t.power.data()};
+    return frozen_render_impl<double>(c, p, rounds, pr, threads, img1, flux4, radiance4);
+}
+
+/* The analytic gradient of L(θ) = Σ g · F(θ) at θ = (mats1, lights1), in double, by forward-mode
+ * dual numbers (phx_dual.hpp): θ is laid out as 4 per material (base colour r, g, b, roughness),
+ * then 3 per light (power r, g, b); g_img holds npx x 3 doubles; grad receives the θ-sized
+ * gradient and *loss (optional) L.  The parameters are seeded DUAL_CHUNK at a time, one frozen
+ * evaluation per chunk. */
+constexpr int DUAL_CHUNK = 8;
+__attribute__((visibility("default"))) int orc_frozen_grad(void *o, const phx_params *p, uint32_t rounds,
+                                                          const phx_material *mats1, uint32_t n_mats,
+                                                          const phx_light *lights1, uint32_t n_lights,
+                                                          const double *g_img, int threads, double *grad,
+                                                          double *loss) {
+    auto *c = (OrcCtx *)o;
+    if (!c || !p || !g_img || !grad || rounds == 0 || n_mats != c->n_materials || n_lights != c->sc.n_lights ||
+        (n_mats && !mats1) || (n_lights && !lights1))
+        return PHX_E_INVALID;
+    using DD = Dual<DUAL_CHUNK>;
+    const u32 np = 4 * n_mats + 3 * n_lights, npx = p->width * p->height;
+    std::vector<DD> img((size_t)npx * 3);
+    for (u32 c0 = 0; c0 < np; c0 += DUAL_CHUNK) {
+        std::vector<V4<DD>> base(n_mats), power(n_lights);
+        std::vector<DD> rough(n_mats);
+        auto seeded = [&](double v, u32 param) {
+            DD d(v);
+            if (param >= c0 && param < c0 + DUAL_CHUNK)
+                d.d[param - c0] = 1.0;
+            return d;
+        };
+        for (u32 m = 0; m < n_mats; m++) {
+            const phx_f4 &b = mats1[m].base_color;
+            base[m] = mk<DD>(seeded(b.x, 4 * m), seeded(b.y, 4 * m + 1), seeded(b.z, 4 * m + 2), DD((double)b.w));
+            rough[m] = seeded(mats1[m].roughness, 4 * m + 3);
+        }
+        for (u32 l = 0; l < n_lights; l++) {
+            const phx_f4 &w = lights1[l].power;
+            const u32 k = 4 * n_mats + 3 * l;
+            power[l] = mk<DD>(seeded(w.x, k), seeded(w.y, k + 1), seeded(w.z, k + 2), DD((double)w.w));
+        }
+        frozen::Primed<DD> pr{mats1, lights1, base.data(), rough.data(), power.data()};
+        int r = frozen_render_impl<DD>(c, p, rounds, pr, threads, img.data(), nullptr, nullptr);
+        if (r)
+            return r;
+        double l = 0.0;
+        double acc[DUAL_CHUNK] = {};
+        for (size_t i = 0; i < img.size(); i++) {
+            l += g_img[i] * img[i].v;
+            for (int j = 0; j < DUAL_CHUNK; j++)
+                acc[j] += g_img[i] * img[i].d[j];
+        }
+        for (u32 j = 0; j < DUAL_CHUNK && c0 + j < np; j++)
+            grad[c0 + j] = acc[j];
+        if (loss)
+            *loss = l;
+    }
+    return PHX_OK;
 }
 
 __attribute__((visibility("default"))) int orc_image(const void *flux4, const void *radiance4, uint32_t n, int prec,

@@ -130,8 +130,8 @@ class SceneSpec(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("trace_block", "emit_block", "gather_block", "trace_blocks_per_sm",
                                           "emit_blocks_per_sm", "persistent", "nee_wavefront",
-                                          "concurrent_passes", "gather_sorted", "pipeline_rounds")] + \
-               [("reserved", C.c_uint32 * 2)]
+                                          "concurrent_passes", "gather_sorted", "pipeline_rounds", "gather_coop")] + \
+               [("reserved", C.c_uint32 * 1)]
 
 
 SIZES = {Triangle: 176, Material: 96, UvTransformBlock: 192, Light: 128, CameraParams: 112, BvhNode: 32,

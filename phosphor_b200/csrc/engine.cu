@@ -442,6 +442,7 @@ int Engine::create(const phx_scene *scenes, const phx_params *params, uint32_t n
     tune.nee_wavefront = 1;
     tune.concurrent_passes = 0;
     tune.gather_sorted = 1;
+    tune.gather_coop = 1;
     tune.pipeline_rounds = 2; // two rounds in flight per graph replay (measured faster, bit-identical)
     for (uint32_t i = 0; i < n; i++)
         if (params[i].flags & PHX_F_SIMPLE_TRAVERSAL)
@@ -626,7 +627,7 @@ void Engine::enq_gather_r(RoundSet &R, cudaStream_t s) {
     GatherBufs g{R.hp[0], R.hp[1], R.hp[2], R.hp[3], R.hp[4], R.hp[5], R.s_posdir, R.s_power, R.s_dir, R.s_pow,
                  R.cell_start, (u32)max_photons, flux.as<float4>(), weight.as<float>(), radiance.as<float4>(), rec_r2,
                  rec_ratio, order};
-    launch_gather(lc(R), g, (int)tune.gather_block, s);
+    launch_gather(lc(R), g, (int)tune.gather_block, tune.gather_coop != 0, s);
     ev(ST_GATHER, true, s);
 }
 
@@ -1120,6 +1121,7 @@ int Engine::autotune(uint32_t rounds, phx_tuning *chosen) {
     }
     knob(&phx_tuning::concurrent_passes, {0u, 1u});
     knob(&phx_tuning::gather_sorted, {1u, 0u});
+    knob(&phx_tuning::gather_coop, {1u, 0u});
     // rounds in flight: each more needs another set of per-round buffers; a candidate whose sets do
     // not fit in device memory is skipped
     for (uint32_t v : {1u, 2u, 4u}) {

@@ -144,6 +144,159 @@ __global__ void __launch_bounds__(128, PHX_GATHER_MINB) k_gather(LaunchCtx lc, G
         gather_pixel(lc.scenes[s], gid, g);
 }
 
+// Cooperative form of the same gather.  The pixels arrive grouped by photon-grid cell (k_pixel_keys),
+// so the lanes of a warp mostly need the same cells.  For each of the 27 neighbour offsets the warp
+// forms groups of lanes that need the same (global) cell; for each group all 32 lanes load the
+// cell's photon records 32 at a time — one coalesced 16-byte load per lane per record array — into
+// the warp's shared-memory stage, and the lanes of the group walk the staged records in order.  A
+// pixel still sums its cells in the reference's order and each cell in sorted (canonical) order
+// with the same operations, so its result is the per-thread kernel's bit for bit; what changes is
+// that one load round trip now serves 32 records instead of one.
+constexpr u32 COOP_WARPS = 4;
+#ifndef PHX_GATHER_STAGE_ALL
+#define PHX_GATHER_STAGE_ALL 1 // stage the decoded direction and power too (else load them per lane)
+#endif
+
+__global__ void __launch_bounds__(32 * COOP_WARPS, PHX_GATHER_MINB) k_gather_coop(LaunchCtx lc, GatherBufs g) {
+    __shared__ float4 st_pd[COOP_WARPS][32];
+#if PHX_GATHER_STAGE_ALL
+    __shared__ float4 st_dir[COOP_WARPS][32];
+    __shared__ float4 st_pow[COOP_WARPS][32];
+#endif
+    constexpr u32 FULL = 0xffffffffu, NONE = 0xffffffffu;
+    const u32 lane = threadIdx.x & 31u, wq = threadIdx.x >> 5;
+    const u32 gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const SceneDesc *scp = nullptr;
+    u32 gpix = 0;
+    bool gathering = false;
+    float4 pos = zero4(), nrm = zero4(), fso = zero4(), nf = zero4();
+    float wso = 0.0f, r_sq = 0.0f, found = 0.0f, denom = 1.0f, qx = 0.0f, qy = 0.0f, qz = 0.0f;
+    if (gid < lc.total_pixels) {
+        gpix = g.order ? __ldg(&g.order[gid]) : gid;
+        const u32 s = lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gpix);
+        scp = &lc.scenes[s];
+        if (scp->active) {
+            const float4 ge = g.hp_emission[gpix];
+            const float4 rso = g.radiance[gpix];
+            float4 r = f4(ge.x, ge.y, ge.z, 0.0f);
+            if (ge.w == 0.0f) {
+                g.radiance[gpix] = rso + r;
+                if (g.rec_r2) {
+                    g.rec_r2[gpix] = 0.0f;
+                    g.rec_ratio[gpix] = 1.0f;
+                }
+            } else {
+                const float4 direct = g.hp_direct[gpix];
+                r.x += direct.x;
+                r.y += direct.y;
+                r.z += direct.z;
+                g.radiance[gpix] = rso + r;
+                fso = g.flux[gpix];
+                wso = g.weight[gpix];
+                const GridDev &grid = scp->grid;
+                r_sq = fso.w;
+                if (r_sq < EPS) {
+                    float hx = grid.cx * 0.5f, hy = grid.cy * 0.5f, hz = grid.cz * 0.5f;
+                    r_sq = hx * hx + hy * hy + hz * hz;
+                }
+                pos = g.hp_pos[gpix];
+                nrm = g.hp_normal[gpix];
+                denom = 2.0f * r_sq;
+                qx = (pos.x - grid.ox) / grid.cx;
+                qy = (pos.y - grid.oy) / grid.cy;
+                qz = (pos.z - grid.oz) / grid.cz;
+                gathering = true;
+            }
+        }
+    }
+    constexpr float M = 1.0f / 1024.0f;
+    for (u32 i = 0; i < 27; i++) {
+        u32 key = NONE;
+        if (gathering) { // the per-thread kernel's cell and cell-distance tests
+            const GridDev &grid = scp->grid;
+            const i32 ox = (i32)(i % 3) - 1;
+            const i32 oy = (i32)((i / 3) % 3) - 1;
+            const i32 oz = (i32)((i / 9) % 3) - 1;
+            float px = pos.x, py = pos.y, pz = pos.z;
+            px += (float)ox * grid.cx;
+            py += (float)oy * grid.cy;
+            pz += (float)oz * grid.cz;
+            const u32 h = get_hash(px, py, pz, grid);
+            if (h != 0) {
+                const u32 G = grid.g;
+                const u32 hz = (h - 1) % G, hy = ((h - 1) / G) % G, hx = (h - 1) / (G * G);
+                const float gx = fmaxf(fmaxf(((float)hx - M) - qx, qx - ((float)hx + (1.0f + M))), 0.0f) * grid.cx;
+                const float gy = fmaxf(fmaxf(((float)hy - M) - qy, qy - ((float)hy + (1.0f + M))), 0.0f) * grid.cy;
+                const float gz = fmaxf(fmaxf(((float)hz - M) - qz, qz - ((float)hz + (1.0f + M))), 0.0f) * grid.cz;
+                if (!((gx * gx + gy * gy) + gz * gz > r_sq))
+                    key = scp->cell_base + h;
+            }
+        }
+        u32 pending = __ballot_sync(FULL, key != NONE);
+        while (pending) {
+            const u32 cell = __shfl_sync(FULL, key, __ffs(pending) - 1);
+            const u32 grp = __ballot_sync(FULL, key == cell);
+            pending &= ~grp;
+            const bool mine = (grp >> lane) & 1u;
+            const u32 start = min(__ldg(&g.cell_start[cell]), g.n_cap);
+            const u32 end = min(__ldg(&g.cell_start[cell + 1]), g.n_cap);
+            for (u32 base = start; base < end; base += 32) {
+                const u32 k = base + lane;
+                if (k < end) {
+                    st_pd[wq][lane] = __ldg(&g.s_posdir[k]);
+#if PHX_GATHER_STAGE_ALL
+                    st_dir[wq][lane] = __ldg(&g.s_dir[k]);
+                    st_pow[wq][lane] = __ldg(&g.s_pow[k]);
+#endif
+                }
+                __syncwarp();
+                if (mine) {
+                    const u32 n = min(32u, end - base);
+                    for (u32 j = 0; j < n; j++) { // one photon (photon_hash.h:84-101), in sorted order
+                        const float4 p = st_pd[wq][j];
+                        const float dx = pos.x - p.x, dy = pos.y - p.y, dz = pos.z - p.z, dw = pos.w - 0.0f;
+                        const float dsq = ((dx * dx + dy * dy) + dz * dz) + dw * dw;
+                        if (dsq < r_sq) {
+#if PHX_GATHER_STAGE_ALL
+                            const float4 pd = st_dir[wq][j];
+#else
+                            const float4 pd = __ldg(&g.s_dir[base + j]);
+#endif
+                            if (!(dot(pd, nrm) > 0.0f)) {
+                                const float w =
+                                    GAUSS_ALPHA * (1.0f - (1.0f - pm_expf((-GAUSS_BETA) * dsq / denom)) / GAUSS_DENOM);
+#if PHX_GATHER_STAGE_ALL
+                                nf += w * st_pow[wq][j];
+#else
+                                nf += w * __ldg(&g.s_pow[base + j]);
+#endif
+                                found += w;
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+    }
+    if (!gathering)
+        return;
+    if (g.rec_r2) {
+        g.rec_r2[gpix] = r_sq;
+        g.rec_ratio[gpix] = found > 0.0f ? (wso + scp->alpha * found) / (wso + found) : 1.0f;
+    }
+    if (found > 0.0f) {
+        float nw = wso + scp->alpha * found;
+        float ratio = nw / (wso + found);
+        float nr = r_sq * ratio;
+        float4 albedo = g.hp_base_color[gpix];
+        float4 contribution = g.hp_throughput[gpix] * (albedo / PI) * nf;
+        float4 temp = (fso + contribution) * ratio;
+        g.flux[gpix] = f4(temp.x, temp.y, temp.z, nr);
+        g.weight[gpix] = nw;
+    }
+}
+
 // Pixels whose hit points share a photon-grid cell (and an octant of it) visit the same cells and
 // skip the same ones, so gathering them in one warp keeps its lanes in step and lets them share
 // every photon record load.  Pixels without a diffuse hit point (nothing to gather) sort last.
@@ -177,11 +330,14 @@ void launch_pixel_keys(const LaunchCtx &lc, const float4 *hp_pos, const float4 *
         k_pixel_keys<<<(lc.total_pixels + 255) / 256, 256, 0, st>>>(lc, hp_pos, hp_emission, key_bits, keys);
 }
 
-void launch_gather(const LaunchCtx &lc, const GatherBufs &g, int block, cudaStream_t st) {
+void launch_gather(const LaunchCtx &lc, const GatherBufs &g, int block, bool coop, cudaStream_t st) {
     if (lc.total_pixels == 0)
         return;
     (void)block;
-    k_gather<<<(lc.total_pixels + 127) / 128, 128, 0, st>>>(lc, g);
+    if (coop)
+        k_gather_coop<<<(lc.total_pixels + 32 * COOP_WARPS - 1) / (32 * COOP_WARPS), 32 * COOP_WARPS, 0, st>>>(lc, g);
+    else
+        k_gather<<<(lc.total_pixels + 127) / 128, 128, 0, st>>>(lc, g);
 }
 
 // output.cpp:40-50 tone_map and :52-83 apply_tonemap, before/after u8 quantisation

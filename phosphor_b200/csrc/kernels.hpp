@@ -134,7 +134,8 @@ struct GatherBufs {
     float *rec_ratio;      // optional: per pixel, the SPPM ratio applied to the flux (1 if none)
     const u32 *order;      // optional: thread t gathers pixel order[t] (pixels grouped by grid cell)
 };
-void launch_gather(const LaunchCtx &lc, const GatherBufs &g, int block, cudaStream_t st);
+// coop: the warp-cooperative kernel (k_gather_coop), else one thread per pixel (k_gather)
+void launch_gather(const LaunchCtx &lc, const GatherBufs &g, int block, bool coop, cudaStream_t st);
 // Per pixel a sort key that groups hit points by photon-grid cell: ((cell_base + cell) << 3 | octant
 // of the point inside its cell), 0 for pixels without a diffuse hit point.
 void launch_pixel_keys(const LaunchCtx &lc, const float4 *hp_pos, const float4 *hp_emission, u32 key_bits, u32 *keys,

@@ -100,6 +100,19 @@ def config3_specs(n: int = 16, seed: int = 11) -> list[SceneSpec]:
     return out
 
 
+def scaled(spec: SceneSpec, k: int) -> SceneSpec:
+    """A 1/k-scale copy of a scene: resolution divided by k per side and the photon budget by k^2,
+    so that photons per pixel area, the photon grid and the initial radius stay those of the scene."""
+    return dataclasses.replace(spec, width=max(1, spec.width // k), height=max(1, spec.height // k),
+                               photons=max(1, spec.photons // (k * k)))
+
+
+# Calibration of the configs[3] references (long fp32 GPU renders): FP64 oracle renders of 1/8-scale
+# copies of the 16 scenes, RMSE_REF_ROUNDS rounds each with an independent seed
+# (tests/golden/make_config3_fp64_refs.py -> tests/golden/config3_fp64_refs.npz).
+CONFIG3_CAL_SCALE = 8
+
+
 def rmse(a: np.ndarray, b: np.ndarray) -> float:
     d = np.asarray(a, np.float64) - np.asarray(b, np.float64)
     return float(np.sqrt(np.mean(d * d)))

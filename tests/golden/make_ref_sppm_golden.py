@@ -12,7 +12,8 @@ library against the reference itself without a reference checkout:
   a scene with a transmissive surface (with 2 and 16 direct samples), all four light kinds in one
   scene (5 samples), textured materials (base colour, emissive, metal-rough, transmission,
   occlusion and normal maps, non-identity UV transforms, an emissive texture on the area light,
-  Beer-Lambert attenuation), and three glass panes under a point light.
+  Beer-Lambert attenuation), three glass panes under a point light, and a box of rough mirrors
+  whose camera paths outnumber the library's deferred specular-NEE slots.
 
 The lights come from the reference's own constructors (light.cpp) and every light luminance
 prefix sum from its SceneData::build_lum_pref_sum.
@@ -205,6 +206,28 @@ def panes_scene(base: dict) -> dict:
     return with_lights(out, [R.make_light(R.LIGHT_POINT, pos=(0.5, 0.9, 0.5), power=(1.0, 1.0, 1.0))])
 
 
+def mirror_scene(base: dict) -> dict:
+    """The back, left and right walls rough mirrors (floor and ceiling stay diffuse, so photons are
+    stored): camera paths bounce between the mirrors with a specular event at nearly every bounce,
+    more events than the library's deferred specular-NEE sample slots hold (one per pixel and
+    sample), so many take its traced-in-place fallback."""
+    tris = structs(base["tris"], A.Triangle)
+    mats = list(structs(base["mats"], A.Material))
+    uvs = list(structs(base["uvs"], A.UvTransformBlock))
+    mirror = A.Material.from_buffer_copy(bytes(mats[0]))
+    mirror.metallic, mirror.roughness = 1.0, 0.1
+    mirror.base_color.x, mirror.base_color.y, mirror.base_color.z = 0.95, 0.93, 0.9
+    mats.append(mirror)
+    uvs.append(A.UvTransformBlock.from_buffer_copy(bytes(uvs[0])))
+    for t in tris:
+        if wall_of(t) in ("back", "left", "right"):
+            t.mat_index = len(mats) - 1
+    out = dict(base)
+    out.update(tris=to_raw(tris), mats=np.frombuffer(b"".join(bytes(m) for m in mats), np.uint8),
+               uvs=np.frombuffer(b"".join(bytes(u) for u in uvs), np.uint8))
+    return out
+
+
 PROCEDURAL = [
     # name, kind, detail, width, height, photons, bounces, grid, samples
     ("cornell", A.PHX_SCENE_CORNELL, 0, 32, 32, 4096, 8, 50, 4),
@@ -218,6 +241,7 @@ CUSTOM = [
     ("cornell_mixed_lights", A.PHX_SCENE_CORNELL, 0, mixed_scene, 4096, 8, 50, 5),
     ("cornell_textured", A.PHX_SCENE_CORNELL, 0, textured_scene, 4096, 8, 50, 4),
     ("panes_point", A.PHX_SCENE_CORNELL, 0, panes_scene, 4096, 8, 50, 16),
+    ("mirror_box", A.PHX_SCENE_CORNELL, 0, mirror_scene, 4096, 8, 50, 16),
 ]
 
 

@@ -2,11 +2,14 @@
 
 The function differentiated is the frozen-path estimator F(θ) (include/phx.h, oracle/phx_frozen.hpp):
 paths and every discrete choice come from the scene's own parameters θ0, only weights move with θ.
-The oracle evaluates F in double; its central finite differences (h = 1e-3, frozen random numbers)
-are the reference gradient.  Gradients must agree within GRAD_TOL = 1e-3 relative.
+The oracle evaluates F in double, and two reference gradients come from it: central finite
+differences (h = 1e-3, frozen random numbers) and the analytic FP64 gradient, forward-mode dual
+numbers through the same evaluation (oracle/phx_dual.hpp), which gives every one of the 131
+partial derivatives exactly.  Gradients must agree within GRAD_TOL = 1e-3 relative.
 
-CPU tests pin the oracle's F: its θ0 replay is bit-identical to the float render, and F is smooth.
-GPU tests compare the library's adjoint (phx_adjoint_backward) with the finite differences.
+CPU tests pin the oracle: its θ0 replay is bit-identical to the float render, F is smooth, and the
+analytic gradient equals the finite differences.  GPU tests compare the library's adjoint
+(phx_adjoint_backward) with both, the analytic one on all 131 coordinates.
 """
 import numpy as np
 import pytest
@@ -84,6 +87,55 @@ def test_frozen_estimator_is_smooth():
     f1, _ = fd_directional(o, args, t, th, d, g)
     f2, _ = fd_directional(o, args, t, th, d / 2, g)
     assert abs(f1 - 2 * f2) <= 1e-4 * abs(f1)
+
+
+def test_analytic_gradient_equals_finite_differences():
+    """The forward-mode FP64 gradient of L(θ) = Σ g·F(θ) equals central differences of F along
+    random directions through all parameters and along single coordinates (the finite differences
+    carry an O(h^2) truncation error, about 1e-6 relative here)."""
+    scene, args = small_atrium()
+    o = O.Oracle(scene)
+    t = ParamTable(scene.materials(), scene.lights())
+    th = t.vector().astype(np.float64)
+    rng = np.random.default_rng(4)
+    g = rng.standard_normal(args.width * args.height * 3)
+    grad, loss = o.frozen_grad(args.params(), ROUNDS, scene.materials(), scene.lights(), g)
+    assert loss == pytest.approx(loss_of(o, args, t, th.astype(np.float32), g), rel=1e-12)
+    assert grad.shape == (t.size,) and (grad != 0).sum() > 0.9 * t.size
+    interior = (th[3:4 * t.n_mat:4] > 0.01) & (th[3:4 * t.n_mat:4] < 0.99)
+    for k in range(3):
+        d = rng.standard_normal(th.size)
+        d[3:4 * t.n_mat:4] *= interior
+        fd, step = fd_directional(o, args, t, th, d, g)
+        assert abs(float(np.dot(grad, step)) - fd) <= 1e-4 * abs(fd), k
+    for i in list(np.argsort(-np.abs(grad))[:4]) + [4 * t.n_mat + 2]:
+        d = np.zeros(th.size)
+        d[i] = 1.0
+        fd, step = fd_directional(o, args, t, th, d, g)
+        assert abs(grad[i] * step[i] - fd) <= 1e-4 * abs(fd) + 1e-12, i
+
+
+@pytest.mark.gpu
+def test_adjoint_matches_the_analytic_gradient_on_every_coordinate():
+    """The library's reverse-mode adjoint against the oracle's forward-mode FP64 gradient, all 131
+    coordinates: each within GRAD_TOL relative, or within GRAD_TOL of the largest partial for
+    coordinates that are nearly zero (float accumulation noise)."""
+    scene, args = small_atrium()
+    t = ParamTable(scene.materials(), scene.lights())
+    rng = np.random.default_rng(5)
+    g = rng.standard_normal(args.width * args.height * 3).astype(np.float32)
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        r.adjoint_forward(ROUNDS)
+        grad = r.adjoint_backward(g).astype(np.float64)
+    want, _ = O.Oracle(scene).frozen_grad(args.params(), ROUNDS, scene.materials(), scene.lights(),
+                                          g.astype(np.float64))
+    assert grad.shape == want.shape == (t.size,)
+    scale = np.abs(want).max()
+    err = np.abs(grad - want)
+    bad = np.flatnonzero(err > GRAD_TOL * np.maximum(np.abs(want), 1e-3 * scale))
+    assert len(bad) == 0, [(int(i), grad[i], want[i]) for i in bad[:8]]
+    assert np.count_nonzero(want) > 0.9 * t.size
 
 
 @pytest.mark.gpu

@@ -243,6 +243,44 @@ def test_kernel_forms_agree(name):
             assert np.array_equal(o[b], outs[0][b]), b
 
 
+@pytest.mark.parametrize("sorted_pixels", [1, 0])
+@pytest.mark.parametrize("name", list(SCENES))
+def test_cooperative_gather_equals_the_per_thread_gather(name, sorted_pixels):
+    """The warp-cooperative gather (records staged in shared memory per cell group) and the
+    one-thread-per-pixel gather give identical bits, with the pixels grouped by cell or in plain
+    order (where most warps need several cells per neighbour offset)."""
+    scene, args = make(name)
+    outs = []
+    for coop in (0, 1):
+        with P.Renderer(args) as r:
+            r.set_scene(scene)
+            t = r.tuning()
+            t.gather_coop, t.gather_sorted = coop, sorted_pixels
+            r.set_tuning(t)
+            r.iterate(3)
+            outs.append({b: r.read(b).view(np.uint32).copy() for b in ["FLUX", "PHOTON_WEIGHT", "RADIANCE"]})
+    for b in outs[0]:
+        assert np.array_equal(outs[0][b], outs[1][b]), b
+    assert (outs[0]["PHOTON_WEIGHT"].view(np.float32) > 0).mean() > 0.1
+
+
+def test_cooperative_gather_in_a_batch():
+    """Lanes of one warp may belong to different scenes of a batch: cells are grouped by their
+    global index, so the cooperative gather equals the per-thread one there too."""
+    made = [make(n, photons_per_round=1 << 12) for n in ("cornell", "caustic", "atrium")]
+    outs = []
+    for coop in (0, 1):
+        batch = P.Batch([s for s, _ in made], [a for _, a in made])
+        t = batch.tuning()
+        t.gather_coop = coop
+        batch.set_tuning(t)
+        batch.iterate(2, graph=True)
+        outs.append([batch.read(i, "FLUX").view(np.uint32).copy() for i in range(3)])
+        batch.close()
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("name", list(SCENES))
 def test_traversal_tree_does_not_change_results(name):
     """Traversing the reference median-split tree or binned-SAH trees with 1, 4 or 8 triangles per

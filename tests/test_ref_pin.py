@@ -45,7 +45,7 @@ def image_u8(flux, radiance, total, rounds):
 
 def test_fixture_covers_the_scene_kinds_and_light_kinds():
     assert set(CASES) == {"cornell", "caustic", "atrium", "caustic_spot", "caustic_directional",
-                          "cornell_mixed_lights", "cornell_textured", "panes_point"}
+                          "cornell_mixed_lights", "cornell_textured", "panes_point", "mirror_box"}
     for c in CASES.values():
         assert len(c["r1_photon_pos"]) > 500 and (c["r1_hp"][:, 5, 3] == 1.0).mean() > 0.2
 
