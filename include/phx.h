@@ -213,7 +213,9 @@ enum {
     PHX_BUF_EMIT_COUNT = 19,   /* u32 photons stored by each emitted photon path */
     PHX_BUF_BVH_NODES = 20,    /* phx_bvh_node, reference layout */
     PHX_BUF_SORT_PERM = 21,    /* u32 canonical index of each cell-ordered photon */
-    PHX_BUF__COUNT = 22
+    PHX_BUF_ROUND_RNG = 22,    /* u32: the state of the round-seed PCG stream (Renderer::rng, renderer.cpp:49,65);
+                                  writing a saved state makes the following rounds reuse its seeds */
+    PHX_BUF__COUNT = 23
 };
 
 /* ---- context lifecycle -------------------------------------------------------------------- */

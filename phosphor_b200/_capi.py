@@ -29,14 +29,14 @@ PHX_F_DEFAULT, PHX_F_SIMPLE_TRAVERSAL, PHX_F_REFERENCE_BVH, PHX_F_BINARY_BVH = 0
 BUFFERS = ["HP_POS", "HP_NORMAL", "HP_THROUGHPUT", "HP_BASE_COLOR", "HP_DIRECT", "HP_EMISSION", "FLUX",
            "PHOTON_WEIGHT", "RADIANCE", "PHOTON_POS", "PHOTON_POWER", "PHOTON_DIR", "PHOTON_HASH", "CELL_COUNT",
            "CELL_START", "CELL_END", "SORTED_POS", "SORTED_POWER", "SORTED_DIR", "EMIT_COUNT", "BVH_NODES",
-           "SORT_PERM"]
+           "SORT_PERM", "ROUND_RNG"]
 BUF = {name: i for i, name in enumerate(BUFFERS)}
 # numpy element layout of each buffer (reference layout)
 BUF_DTYPE = {name: (np.float32, 4) for name in ["HP_POS", "HP_NORMAL", "HP_THROUGHPUT", "HP_BASE_COLOR", "HP_DIRECT",
                                                  "HP_EMISSION", "FLUX", "RADIANCE", "PHOTON_POS", "SORTED_POS"]}
 BUF_DTYPE.update({name: (np.uint32, 1) for name in ["PHOTON_POWER", "PHOTON_DIR", "PHOTON_HASH", "CELL_COUNT",
                                                      "CELL_START", "CELL_END", "SORTED_POWER", "SORTED_DIR",
-                                                     "EMIT_COUNT", "SORT_PERM"]})
+                                                     "EMIT_COUNT", "SORT_PERM", "ROUND_RNG"]})
 BUF_DTYPE["PHOTON_WEIGHT"] = (np.float32, 1)
 BUF_DTYPE["BVH_NODES"] = (np.float32, 8)
 

@@ -1236,6 +1236,9 @@ int Engine::read_buffer(uint32_t s, int which, void *dst, uint64_t off, uint64_t
     case PHX_BUF_BVH_NODES:
         bd = {sizeof(phx_bvh_node), sc[s].nodes.size()};
         break;
+    case PHX_BUF_ROUND_RNG:
+        bd = {4, 1};
+        break;
     default:
         return fail(PHX_E_INVALID, "unknown buffer id");
     }
@@ -1317,6 +1320,9 @@ int Engine::read_buffer(uint32_t s, int which, void *dst, uint64_t off, uint64_t
         std::memcpy(tmp.data(), sc[s].nodes.data() + e0, sizeof(phx_bvh_node) * ne);
         r = PHX_OK;
         break;
+    case PHX_BUF_ROUND_RNG:
+        r = dcopy(d_rng.as<u32>() + s, 4);
+        break;
     case PHX_BUF_SORT_PERM:
         if (!(r = fetch32(perm + poff + e0, v)))
             for (uint64_t i = 0; i < ne; i++)
@@ -1375,6 +1381,8 @@ int Engine::write_buffer(uint32_t s, int which, const void *src, uint64_t off, u
     case PHX_BUF_CELL_START:
         stage_state |= 4;
         return put(cell_start.p, 4 * (size_t)d.n_cells);
+    case PHX_BUF_ROUND_RNG:
+        return put(d_rng.p, 4);
     case PHX_BUF_PHOTON_POWER: case PHX_BUF_PHOTON_DIR: case PHX_BUF_SORTED_POS: case PHX_BUF_SORTED_DIR: {
         const bool sorted = which == PHX_BUF_SORTED_POS || which == PHX_BUF_SORTED_DIR;
         const size_t es = which == PHX_BUF_SORTED_POS ? 16 : 4;

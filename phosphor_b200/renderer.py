@@ -271,7 +271,7 @@ class Renderer:
         info = self.info()
         dt, width = A.BUF_DTYPE[name]
         count = {"CELL_COUNT": info.bucket_count, "CELL_START": info.bucket_count, "CELL_END": info.bucket_count,
-                 "EMIT_COUNT": info.photons_per_round, "BVH_NODES": info.n_bvh_nodes}.get(name)
+                 "EMIT_COUNT": info.photons_per_round, "BVH_NODES": info.n_bvh_nodes, "ROUND_RNG": 1}.get(name)
         if count is None:
             count = info.n_pixels if name.startswith("HP_") or name in ("FLUX", "RADIANCE", "PHOTON_WEIGHT") \
                 else info.n_photons
@@ -444,7 +444,7 @@ class Batch:
         info = self.info(s)
         dt, width = A.BUF_DTYPE[name]
         count = {"CELL_COUNT": info.bucket_count, "CELL_START": info.bucket_count, "CELL_END": info.bucket_count,
-                 "EMIT_COUNT": info.photons_per_round, "BVH_NODES": info.n_bvh_nodes}.get(name)
+                 "EMIT_COUNT": info.photons_per_round, "BVH_NODES": info.n_bvh_nodes, "ROUND_RNG": 1}.get(name)
         if count is None:
             count = info.n_pixels if name.startswith("HP_") or name in ("FLUX", "RADIANCE", "PHOTON_WEIGHT") \
                 else info.n_photons

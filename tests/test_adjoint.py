@@ -234,3 +234,19 @@ def test_torch_function_and_a_descent_step():
             th1 = th - 0.02 * th.grad / th.grad.abs().max()
             loss1 = ((img_of(th1) - target) ** 2).sum()
     assert float(loss1.detach()) < float(loss0.detach())
+
+
+@pytest.mark.gpu
+def test_round_rng_state_replays_the_seeds():
+    """PHX_BUF_ROUND_RNG holds the round-seed stream: a render after writing a saved state back
+    repeats the earlier render bit for bit; without it the next render draws new seeds."""
+    scene, args = small_atrium()
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        s0 = r.read("ROUND_RNG").copy()
+        a = r.adjoint_forward(ROUNDS)
+        b = r.adjoint_forward(ROUNDS)
+        r.write("ROUND_RNG", s0)
+        c = r.adjoint_forward(ROUNDS)
+    assert not np.array_equal(a, b)
+    assert np.array_equal(a.view(np.uint32), c.view(np.uint32))
