@@ -223,3 +223,34 @@ def gpu_reference(spec: SceneSpec, rounds: int, seed_offset: int = 1000003, devi
     img = r.image()
     r.close()
     return img
+
+
+def batch_images(specs, rounds: int, seed_offset: int = 0, device: int = 0,
+                 pipeline: int = PIPELINE_ROUNDS) -> list[np.ndarray]:
+    """Images of the scenes after `rounds` rounds advanced together in the graph form, each scene's
+    round seeds drawn from scene seed + seed_offset (an independent stream for seed_offset != 0)."""
+    b = Batch([s.scene() for s in specs], [s.args(seed=s.seed + seed_offset) for s in specs], device=device)
+    t = b.tuning()
+    t.pipeline_rounds = pipeline
+    b.set_tuning(t)
+    b.iterate(rounds, graph=True)
+    imgs = [b.image(i) for i in range(len(specs))]
+    b.close()
+    return imgs
+
+
+def time_plain_run(spec: SceneSpec, rounds: int, device: int = 0) -> tuple[float, np.ndarray]:
+    """Wall seconds of `rounds` rounds of one scene in the plain per-pass form (per-pass launches and
+    the reference's two host syncs per round, renderer.cpp:64-86), end to end from a fresh SPPM
+    state with the scene set up beforehand, and the image it reaches."""
+    r = Renderer(spec.args(), device=device)
+    r.set_scene(spec.scene())
+    r.sync()
+    t0 = time.perf_counter()
+    for _ in range(rounds):
+        r.round()
+    r.sync()
+    dt = time.perf_counter() - t0
+    img = r.image()
+    r.close()
+    return dt, img
