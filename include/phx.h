@@ -293,6 +293,28 @@ typedef struct phx_scene_spec {
 PHX_API int phx_scene_generate(const phx_scene_spec *spec, phx_scene *out, void **handle);
 PHX_API int phx_scene_free(void *handle);
 
+/* ---- glTF 2.0 scene ingest (src/parsers/scene.cpp:206-233 read_gltf_scene, material.cpp:157-184,
+ * texture.cpp:19-92) -------------------------------------------------------------------------
+ * Loads a .gltf (with .bin files or data URIs) or .glb file into library-owned host arrays and
+ * fills *out like phx_scene_generate (free with phx_scene_free).  The reference reads the file
+ * through assimp; this reads the glTF document directly with the same conversions: node
+ * transforms, one material per mesh primitive, emissive primitives as area lights of power
+ * π·emissive·area, KHR_lights_punctual power = colour·intensity/683, perspective cameras
+ * (hfov = 2·atan(aspect·tan(yfov/2))), KHR materials transmission / ior / volume / emissive
+ * strength, KHR_texture_transform, PNG textures as 8-bit RGB (other image formats are skipped:
+ * the material then has no texture).  The camera `camera` (the reference takes the first) gets
+ * the render's aspect width/height (when both are nonzero) and focus(defocus_angle,
+ * focus_distance) (renderer.cpp:24-28).  PHX_E_INVALID (with the reason in phx_last_error) for
+ * an unreadable file, a malformed document, a scene without triangles or without that camera. */
+typedef struct phx_gltf_options {
+    uint32_t width, height;   /* render size (0, 0: the camera's own aspect) */
+    float defocus_angle;      /* --defocus-angle (degrees) */
+    float focus_distance;     /* --focus-distance (0 = 1) */
+    uint32_t camera;          /* camera index in traversal order (0 = the reference's choice) */
+    uint32_t reserved[3];
+} phx_gltf_options;
+PHX_API int phx_scene_load_gltf(const char *path, const phx_gltf_options *options, phx_scene *out, void **handle);
+
 /* ---- batched scenes: one launch per stage for many scenes ---------------------------------- */
 /* Creates one engine over n scenes with per-scene params (uneven sizes allowed). */
 PHX_API int phx_batch_create(const phx_scene *scenes, const phx_params *params, uint32_t n, int device,

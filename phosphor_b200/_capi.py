@@ -122,6 +122,11 @@ class Info(C.Structure):
                 ("spec_samples", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
+class GltfOptions(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("defocus_angle", C.c_float),
+                ("focus_distance", C.c_float), ("camera", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+
+
 class SceneSpec(C.Structure):
     _fields_ = [("kind", C.c_int), ("seed", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32),
                 ("detail", C.c_uint32), ("reserved", C.c_uint32 * 5)]
@@ -162,6 +167,7 @@ PROTOTYPES = [
     ("phx_lum_pref_sum", C.c_int, [C.POINTER(Light), C.c_uint32, C.POINTER(C.c_float)]),
     ("phx_scene_generate", C.c_int, [C.POINTER(SceneSpec), C.POINTER(Scene), C.POINTER(VP)]),
     ("phx_scene_free", C.c_int, [VP]),
+    ("phx_scene_load_gltf", C.c_int, [C.c_char_p, C.POINTER(GltfOptions), C.POINTER(Scene), C.POINTER(VP)]),
     ("phx_batch_create", C.c_int, [C.POINTER(Scene), C.POINTER(Params), C.c_uint32, C.c_int, C.POINTER(VP)]),
     ("phx_batch_destroy", C.c_int, [VP]),
     ("phx_batch_iterate", C.c_int, [VP, C.c_uint32, C.c_int]),

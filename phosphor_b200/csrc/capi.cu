@@ -235,6 +235,26 @@ PHX_API int phx_scene_generate(const phx_scene_spec *spec, phx_scene *out, void 
     });
 }
 
+PHX_API int phx_scene_load_gltf(const char *path, const phx_gltf_options *options, phx_scene *out, void **handle) {
+    return guard([&]() -> int {
+        if (!path || !out || !handle)
+            return fail(PHX_E_INVALID, "null argument");
+        phx_gltf_options opt{};
+        if (options)
+            opt = *options;
+        auto *h = new SceneHandle();
+        std::string err;
+        int r = scene_load_gltf(path, opt, h->store, err);
+        if (r) {
+            delete h;
+            return fail(r, err);
+        }
+        h->store.view(out);
+        *handle = h;
+        return PHX_OK;
+    });
+}
+
 PHX_API int phx_scene_free(void *handle) {
     return guard([&]() -> int {
         if (!handle)

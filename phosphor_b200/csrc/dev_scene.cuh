@@ -93,7 +93,10 @@ struct Hit {
     i32 tri; // device triangle index (leaf rank), -1 = none
 };
 
-constexpr int TRAV_STACK = 64;
+#ifndef PHX_TRAV_STACK
+#define PHX_TRAV_STACK 64
+#endif
+constexpr int TRAV_STACK = PHX_TRAV_STACK;
 constexpr u32 LEAF_FIRST_BITS = 27; // leaf reference: ~(first | (count-1) << 27)
 
 // Möller–Trumbore test of hit.h:45-78 with the reference's dot(float4) including w terms.

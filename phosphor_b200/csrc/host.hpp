@@ -62,6 +62,9 @@ struct SceneStore {
 
 int scene_generate(const phx_scene_spec &spec, SceneStore &out, std::string &err);
 
+// read_gltf_scene (src/parsers/scene.cpp:206-233) over a glTF 2.0 document (gltf.cpp)
+int scene_load_gltf(const char *path, const phx_gltf_options &opt, SceneStore &out, std::string &err);
+
 // Camera::Camera + focus + to_params (src/renderer/camera.cpp:3-56)
 int camera_make(const float pos[3], const float at[3], const float up[3], float hfov, float aspect, float defocus,
                 float focus, phx_camera_params *out);

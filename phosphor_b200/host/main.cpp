@@ -1,8 +1,9 @@
 // main.cpp — phx_render: the reference's command line (src/main.cpp:12-61) over libphx.so,
-// rendering one of the procedural scenes (the reference's .glb assets are not available).
+// rendering a glTF 2.0 scene (-m) or one of the procedural scenes.
 #include <chrono>
 #include <cstdio>
 #include <iostream>
+#include <memory>
 
 #include "renderer.hpp"
 
@@ -21,7 +22,10 @@ int main(int argc, char **argv) {
     try {
         int kind = args.scene == "cornell" ? PHX_SCENE_CORNELL : args.scene == "caustic" ? PHX_SCENE_CAUSTIC
                                                                                            : PHX_SCENE_ATRIUM;
-        SceneData scene(kind, args.seed, args.width, args.height, args.scene_detail);
+        std::unique_ptr<SceneData> owned =
+            args.model.empty() ? std::make_unique<SceneData>(kind, args.seed, args.width, args.height, args.scene_detail)
+                               : std::make_unique<SceneData>(args.model, args);
+        const SceneData &scene = *owned;
         Renderer renderer(args, args.output_dir);
         auto t0 = std::chrono::steady_clock::now();
         renderer.set_scene(scene);
@@ -33,7 +37,7 @@ int main(int argc, char **argv) {
         double render = std::chrono::duration<double>(t2 - t1).count();
         std::printf("%s: %u triangles, %ux%u px, %u rounds x %u photons in %.3fs (set_scene %.3fs): %.2f Mphotons/s, "
                     "%u photons stored last round\n",
-                    args.scene.c_str(), scene.scene().n_triangles, info.width, info.height, rounds,
+                    args.model.empty() ? args.scene.c_str() : args.model.c_str(), scene.scene().n_triangles, info.width, info.height, rounds,
                     info.photons_per_round, render, setup,
                     rounds ? (double)rounds * info.photons_per_round / render / 1e6 : 0.0, info.n_photons);
     } catch (const Error &e) {

@@ -39,7 +39,8 @@ std::string usage() {
            "  --sppm-rounds <u32>      number of SPPM rounds (64)\n"
            "  --sppm-alpha <f>         radius reduction ratio (0.7)\n"
            "  --direct-samples <1..128> direct-lighting samples per pixel per round (16)\n"
-           "  --scene <cornell|caustic|atrium> [--detail n]   procedural scene (in place of -m)\n"
+           "  -m <file.glb|file.gltf>  glTF 2.0 scene to render\n"
+           "  --scene <cornell|caustic|atrium> [--detail n]   procedural scene (when no -m is given)\n"
            "  -o <dir>                 output directory\n"
            "  --snapshots              also write images at power-of-two rounds\n"
            "  --plain                  per-pass launches with host syncs (default: graph replay)\n"
@@ -102,6 +103,8 @@ ArgsList parse_args(int argc, char **argv) {
             a.sppm_alpha = f32v(need(i), "--sppm-alpha");
         else if (f == "--direct-samples")
             a.direct_samples = u32v(need(i), 1, 128, "--direct-samples");
+        else if (f == "-m")
+            a.model = need(i);
         else if (f == "--scene")
             a.scene = need(i);
         else if (f == "--detail")
@@ -130,6 +133,15 @@ SceneData::SceneData(int kind, uint32_t seed, uint32_t width, uint32_t height, u
     spec.height = height;
     spec.detail = detail;
     check(phx_scene_generate(&spec, &scene_, &handle_));
+}
+
+SceneData::SceneData(const std::string &gltf_path, const ArgsList &args) {
+    phx_gltf_options opt{};
+    opt.width = args.width;
+    opt.height = args.height;
+    opt.defocus_angle = args.defocus_angle;
+    opt.focus_distance = args.focus_distance;
+    check(phx_scene_load_gltf(gltf_path.c_str(), &opt, &scene_, &handle_));
 }
 
 SceneData::~SceneData() {

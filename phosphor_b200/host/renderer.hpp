@@ -34,7 +34,8 @@ struct ArgsList {
     uint32_t sppm_rounds = 64;
     float sppm_alpha = 0.7f;
     uint32_t direct_samples = 16;
-    std::string scene = "cornell"; // procedural scene in place of -m model.glb
+    std::string model;             // -m: a .glb / .gltf scene file (read_gltf_scene)
+    std::string scene = "cornell"; // procedural scene when no -m is given
     uint32_t scene_detail = 0;
     std::string output_dir = "./phosphor_output";
     bool save_snapshots = false;
@@ -58,6 +59,8 @@ class Error : public std::runtime_error {
 class SceneData {
   public:
     SceneData(int kind, uint32_t seed, uint32_t width, uint32_t height, uint32_t detail = 0);
+    // a glTF 2.0 file (scene.cpp:206-233) with the render size and focus of `args` (renderer.cpp:24-28)
+    SceneData(const std::string &gltf_path, const ArgsList &args);
     ~SceneData();
     SceneData(const SceneData &) = delete;
     SceneData &operator=(const SceneData &) = delete;

@@ -84,6 +84,19 @@ class SceneData:
         A.check(lib.phx_scene_generate(C.byref(spec), C.byref(sc), C.byref(h)))
         return cls(sc, owner=h)
 
+    @classmethod
+    def load_gltf(cls, path: str | os.PathLike, width: int = 0, height: int = 0, defocus_angle: float = 0.0,
+                  focus_distance: float = 1.0, camera: int = 0) -> "SceneData":
+        """read_gltf_scene (src/parsers/scene.cpp:206-233) for a .gltf or .glb file, with the
+        render size's aspect and the focus settings applied to the chosen camera (renderer.cpp:24-28)."""
+        lib = A.load()
+        opt = A.GltfOptions(width=width, height=height, defocus_angle=defocus_angle, focus_distance=focus_distance,
+                            camera=camera)
+        sc = A.Scene()
+        h = C.c_void_p()
+        A.check(lib.phx_scene_load_gltf(os.fsencode(str(path)), C.byref(opt), C.byref(sc), C.byref(h)))
+        return cls(sc, owner=h)
+
     def __del__(self):
         if getattr(self, "_owner", None) is not None and self._owner.value:
             try:

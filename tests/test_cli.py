@@ -73,3 +73,41 @@ def test_cli_render_writes_the_device_image(tmp_path):
         rr.set_scene(scene)
         rr.iterate(5)
         assert np.array_equal(rr.image_u8(), img)
+
+
+def test_missing_model_file_is_an_error(tmp_path):
+    r = run("-m", str(tmp_path / "none.glb"))
+    assert r.returncode == 1 and "cannot read" in r.stderr
+
+
+@pytest.mark.gpu
+def test_cli_renders_a_gltf_scene(tmp_path):
+    """-m renders a .glb through phx_scene_load_gltf; the image equals the Python binding's render
+    of the same loaded scene."""
+    import math
+
+    import phosphor_b200 as P
+    from gltf_writer import Gltf
+    g = Gltf()
+    quad = np.array([[0, 0, 0], [1, 0, 0], [1, 0, 1], [0, 0, 1]], np.float32)
+    idx = np.array([0, 2, 1, 0, 3, 2], np.uint16)
+    floor = g.material(pbrMetallicRoughness={"baseColorFactor": [0.8, 0.7, 0.6, 1.0], "metallicFactor": 0.0})
+    g.node(mesh=g.mesh([{"attributes": {"POSITION": g.accessor(quad)}, "indices": g.accessor(idx, 5123),
+                         "material": floor}]))
+    lamp = g.light(type="point", color=[1.0, 1.0, 1.0], intensity=3000.0)
+    g.node(extensions={"KHR_lights_punctual": {"light": lamp}}, translation=[0.5, 0.8, 0.5])
+    q = [math.sin(-0.6 / 2), 0.0, 0.0, math.cos(-0.6 / 2)]  # look down 0.6 rad
+    g.node(camera=g.camera(0.8, 1.0), translation=[0.5, 0.9, 2.0], rotation=q)
+    g.write_glb(tmp_path / "floor.glb")
+    out = tmp_path / "render"
+    r = run("-m", str(tmp_path / "floor.glb"), "-w", "48", "-h", "40", "-p", "8192", "--max-bounces", "4",
+            "--grid-res", "32", "--sppm-rounds", "3", "--seed", "5", "-o", str(out))
+    assert r.returncode == 0, r.stderr
+    img = read_png(out / "000003.png")
+    scene = P.SceneData.load_gltf(tmp_path / "floor.glb", width=48, height=40)
+    args = P.ArgsList(width=48, height=40, photons_per_round=8192, max_photon_bounces=4, grid_res=32, seed=5)
+    with P.Renderer(args) as rr:
+        rr.set_scene(scene)
+        rr.iterate(3)
+        assert np.array_equal(rr.image_u8(), img)
+    assert img.mean() > 1.0
