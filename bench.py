@@ -356,7 +356,7 @@ def run_batch16(a) -> dict:
 
     import phosphor_b200 as P
     from phosphor_b200 import rmse as R
-    specs = R.config3_specs()
+    specs = R.uneven_batch_specs()
     scenes = [s.scene() for s in specs]
     photons = sum(s.photons for s in specs)
     b = P.Batch(scenes, [s.args() for s in specs])
@@ -398,8 +398,8 @@ def run_batch16(a) -> dict:
             "speedup_vs_plain": round(plain_ms / ms, 3), "stage_ms": stages, "clocks": clk.summary()}
 
 
-# The configs[3] time-to-RMSE study (BASELINE target: graph + batched at least 3x faster than the
-# plain per-pass form).  References: per scene a long fp32 render with an independent seed.
+# The time-to-RMSE study on the 16-scene uneven batch (target: graph + batched at least 3x faster
+# than the plain per-pass form).  References: per scene a long fp32 render with an independent seed.
 TTR_TARGET = 0.01
 TTR_REF_ROUNDS = 1024
 TTR_CHECK = 16
@@ -408,13 +408,13 @@ TTR_CAL_SEED_OFFSET = 2000003  # the calibration renders' seeds: independent of 
 
 
 def time_to_rmse(a) -> dict:
-    """Time to RMSE <= 0.01 on the configs[3] batch: 16 uneven scenes from the three generators
+    """Time to RMSE <= 0.01 on the uneven batch: 16 scenes from the three generators
     (12..291k triangles, 256^2..1024^2 pixels, 2^16..2^21 photons per round, alpha U[0.6, 0.8]).
 
     * reference of each scene: TTR_REF_ROUNDS rounds of a long fp32 render with an independent seed
       (a converged CPU FP64 render at this size is out of reach); its accuracy is calibrated on
       1/8-scale copies of the same scenes, rendered the same way and compared with FP64 oracle
-      renders of those copies (tests/golden/config3_fp64_refs.npz);
+      renders of those copies (tests/golden/batch16_fp64_refs.npz);
     * rounds to target R*_s: the first multiple of TTR_CHECK at which the scene's display image
       (output.cpp:40-76, before quantisation) is within the target of its reference; both forms give
       bit-identical images round by round, so R*_s holds for both; a scene that misses by
@@ -426,12 +426,12 @@ def time_to_rmse(a) -> dict:
     import numpy as np
 
     from phosphor_b200 import rmse as R
-    specs = R.config3_specs()
+    specs = R.uneven_batch_specs()
     t0 = time.perf_counter()
     refs = R.batch_images(specs, TTR_REF_ROUNDS, seed_offset=R.RMSE_REF_SEED_OFFSET)
     t_refs = time.perf_counter() - t0
     cal = None
-    fx = ROOT / "tests" / "golden" / "config3_fp64_refs.npz"
+    fx = ROOT / "tests" / "golden" / "batch16_fp64_refs.npz"
     if fx.exists():
         z = np.load(fx)
         small = [R.scaled(s, int(z["scale"])) for s in specs]
@@ -449,7 +449,7 @@ def time_to_rmse(a) -> dict:
     # the reference's kernel shapes (one thread per item, its median-split tree, NEE inline), per
     # round on a 20-round sample of each scene: a secondary, extrapolated comparison
     t_ref_shape = sum(r * R.time_plain(s, 20, reference_shaped=True) for s, r in zip(specs, r_eff))
-    return {"target_rmse": TTR_TARGET, "workload": "configs[3] batch: 16 scenes, 256^2..1024^2, 2^16..2^21 photons",
+    return {"target_rmse": TTR_TARGET, "workload": "batch of 16 uneven scenes, 256^2..1024^2, 2^16..2^21 photons",
             "reference": f"fp32 GPU render, {TTR_REF_ROUNDS} rounds, independent seed", "reference_s": round(t_refs, 1),
             "calibration": cal, "scenes": len(specs), "check_every": TTR_CHECK, "round_cap": TTR_MAX_ROUNDS,
             "rounds_to_target": r_star, "capped_scenes": capped,
@@ -604,7 +604,7 @@ def main() -> int:
         if not a.no_rmse and out["n_gpus"] == 1 and a.scale == 1:
             out["time_to_rmse"] = time_to_rmse(a)
         if not a.no_inverse and out["n_gpus"] == 1 and a.scale == 1:
-            # configs[4]: inverse rendering through the adjoint (atrium 512x512, 200 Adam steps)
+            # inverse rendering through the adjoint (atrium 512x512, 200 Adam steps)
             inv = run_inverse(a)
             out["inverse"] = {"steps_per_s": inv["value"], "desc": inv["config"]["desc"], **{
                 k: inv["result"][k] for k in ("steps", "n_params", "common_random_numbers", "observed_materials_base",

@@ -79,7 +79,7 @@ def rmse_batch() -> list[SceneSpec]:
     return batch_specs(**RMSE_BATCH)
 
 
-def config3_specs(n: int = 16, seed: int = 11) -> list[SceneSpec]:
+def uneven_batch_specs(n: int = 16, seed: int = 11) -> list[SceneSpec]:
     """The batched workload: n scenes from the three generators with 12 to ~300k triangles,
     resolution in {256^2, 512^2, 1024^2}, 2^16..2^21 photons per round, alpha in U[0.6, 0.8]."""
     rng = np.random.default_rng(seed)
@@ -107,10 +107,10 @@ def scaled(spec: SceneSpec, k: int) -> SceneSpec:
                                photons=max(1, spec.photons // (k * k)))
 
 
-# Calibration of the configs[3] references (long fp32 GPU renders): FP64 oracle renders of 1/8-scale
+# Calibration of the 16-scene batch's references (long fp32 GPU renders): FP64 oracle renders of 1/8-scale
 # copies of the 16 scenes, RMSE_REF_ROUNDS rounds each with an independent seed
-# (tests/golden/make_config3_fp64_refs.py -> tests/golden/config3_fp64_refs.npz).
-CONFIG3_CAL_SCALE = 8
+# (tests/golden/make_batch16_fp64_refs.py -> tests/golden/batch16_fp64_refs.npz).
+BATCH_CAL_SCALE = 8
 
 
 def rmse(a: np.ndarray, b: np.ndarray) -> float:

@@ -1,5 +1,6 @@
-"""Generates tests/golden/config3_fp64_refs.npz: FP64 oracle renders of 1/8-scale copies of the 16
-configs[3] scenes, the calibration of the time-to-RMSE study's references.
+"""Generates tests/golden/batch16_fp64_refs.npz: FP64 oracle renders of 1/8-scale copies of the 16
+scenes of the uneven batch (phosphor_b200.rmse.uneven_batch_specs), the calibration of the time-to-RMSE
+study's references.
 
 At full size (256^2..1024^2 pixels, up to 2^21 photons per round) a converged CPU FP64 render of
 the 16 scenes is out of reach, so the study's references are long fp32 renders on the GPU with an
@@ -11,7 +12,7 @@ RMSE_REF_SEED_OFFSET, through the reference display transform (output.cpp:40-83,
 no ACES).  The bench renders the same 1/8-scale copies with its reference procedure (fp32, GPU,
 another seed) and reports their RMSE to these images.  Images are uint16 fixed point.
 
-    python tests/golden/make_config3_fp64_refs.py [--threads N]
+    python tests/golden/make_batch16_fp64_refs.py [--threads N]
 """
 import argparse
 import sys
@@ -34,8 +35,8 @@ def main():
     a = ap.parse_args()
     imgs = {}
     t_all = time.time()
-    for i, full in enumerate(R.config3_specs()):
-        s = R.scaled(full, R.CONFIG3_CAL_SCALE)
+    for i, full in enumerate(R.uneven_batch_specs()):
+        s = R.scaled(full, R.BATCH_CAL_SCALE)
         t = time.time()
         scene = O.GeneratedScene(s.kind, seed=s.seed, width=s.width, height=s.height, detail=s.detail)
         orc = O.Oracle(scene)
@@ -45,8 +46,8 @@ def main():
         imgs[f"scene{i}"] = np.round(np.clip(img, 0, 1) * 65535).astype(np.uint16).reshape(s.height, s.width, 3)
         print(f"scene {i}: {s.width}x{s.height} kind {s.kind} {s.photons} photons -> {time.time() - t:.1f}s",
               flush=True)
-    out = Path(__file__).with_name("config3_fp64_refs.npz")
-    np.savez_compressed(out, rounds=a.rounds, scale=R.CONFIG3_CAL_SCALE, **imgs)
+    out = Path(__file__).with_name("batch16_fp64_refs.npz")
+    np.savez_compressed(out, rounds=a.rounds, scale=R.BATCH_CAL_SCALE, **imgs)
     print(f"wrote {out} in {time.time() - t_all:.0f}s")
 
 
