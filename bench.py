@@ -399,22 +399,29 @@ def run_batch16(a) -> dict:
 
 
 # The time-to-RMSE study on the 16-scene uneven batch (target: graph + batched at least 3x faster
-# than the plain per-pass form).  References: per scene a long fp32 render with an independent seed.
+# than the plain per-pass form).  At these sizes two independent 1024-round renders still differ by
+# RMSE 0.006-0.014, so the references take 8192 rounds; a second, independent 2048-round set
+# measures their noise.  The whole study takes about 20 GPU-minutes: it runs as --config ttr16.
 TTR_TARGET = 0.01
-TTR_REF_ROUNDS = 1024
-TTR_CHECK = 16
-TTR_MAX_ROUNDS = 1024
+TTR_REF_ROUNDS = 8192
+TTR_REF_CHECK_ROUNDS = 2048
+TTR_CHECK = 32
+TTR_MAX_ROUNDS = 2048
+TTR_PIPELINE = 2               # rounds in flight per graph replay (8 sets of this batch's buffers exceed HBM)
 TTR_CAL_SEED_OFFSET = 2000003  # the calibration renders' seeds: independent of the FP64 images' and the study's
+TTR_CHECK_SEED_OFFSET = 3000017
 
 
-def time_to_rmse(a) -> dict:
-    """Time to RMSE <= 0.01 on the uneven batch: 16 scenes from the three generators
-    (12..291k triangles, 256^2..1024^2 pixels, 2^16..2^21 photons per round, alpha U[0.6, 0.8]).
+def time_to_rmse_batch16(a) -> dict:
+    """Time to RMSE <= 0.01 on the uneven batch: 16 scenes from the three generators (12..291k
+    triangles, 256^2..1024^2 pixels, 2^16..2^21 photons per round, alpha U[0.6, 0.8]).
 
     * reference of each scene: TTR_REF_ROUNDS rounds of a long fp32 render with an independent seed
-      (a converged CPU FP64 render at this size is out of reach); its accuracy is calibrated on
-      1/8-scale copies of the same scenes, rendered the same way and compared with FP64 oracle
-      renders of those copies (tests/golden/batch16_fp64_refs.npz);
+      (a converged CPU FP64 render at this size is out of reach).  Its noise is measured against a
+      second independent render of TTR_REF_CHECK_ROUNDS rounds (RMSE^2 = s_ref^2 + s_check^2 with
+      s_check^2 ~ 4 s_ref^2 for noise falling as rounds^-1/2), and its agreement with double
+      precision on 1/8-scale copies of the same scenes rendered the same way and by the FP64 oracle
+      (tests/golden/batch16_fp64_refs.npz);
     * rounds to target R*_s: the first multiple of TTR_CHECK at which the scene's display image
       (output.cpp:40-76, before quantisation) is within the target of its reference; both forms give
       bit-identical images round by round, so R*_s holds for both; a scene that misses by
@@ -428,14 +435,17 @@ def time_to_rmse(a) -> dict:
     from phosphor_b200 import rmse as R
     specs = R.uneven_batch_specs()
     t0 = time.perf_counter()
-    refs = R.batch_images(specs, TTR_REF_ROUNDS, seed_offset=R.RMSE_REF_SEED_OFFSET)
+    refs = R.batch_images(specs, TTR_REF_ROUNDS, seed_offset=R.RMSE_REF_SEED_OFFSET, pipeline=TTR_PIPELINE)
     t_refs = time.perf_counter() - t0
+    check = R.batch_images(specs, TTR_REF_CHECK_ROUNDS, seed_offset=TTR_CHECK_SEED_OFFSET, pipeline=TTR_PIPELINE)
+    ref_vs_check = [R.rmse(x, y) for x, y in zip(refs, check)]
+    del check
     cal = None
     fx = ROOT / "tests" / "golden" / "batch16_fp64_refs.npz"
     if fx.exists():
         z = np.load(fx)
         small = [R.scaled(s, int(z["scale"])) for s in specs]
-        imgs = R.batch_images(small, TTR_REF_ROUNDS, seed_offset=TTR_CAL_SEED_OFFSET)
+        imgs = R.batch_images(small, TTR_REF_ROUNDS, seed_offset=TTR_CAL_SEED_OFFSET, pipeline=TTR_PIPELINE)
         cal_rmse = [R.rmse(img, z[f"scene{i}"].astype(np.float64) / 65535.0) for i, img in enumerate(imgs)]
         cal = {"scale": int(z["scale"]), "fp64_rounds": int(z["rounds"]), "fp32_rounds": TTR_REF_ROUNDS,
                "rmse_fp32_ref_vs_fp64": [round(x, 5) for x in cal_rmse], "max": round(max(cal_rmse), 5)}
@@ -445,20 +455,61 @@ def time_to_rmse(a) -> dict:
     plain = [R.time_plain_run(s, r) for s, r in zip(specs, r_eff)]
     t_plain = sum(dt for dt, _ in plain)
     plain_rmse = [R.rmse(img, ref) for (_, img), ref in zip(plain, refs)]
-    t_batch = R.time_batched_schedule(specs, r_eff)
+    t_batch = R.time_batched_schedule(specs, r_eff, pipeline=TTR_PIPELINE)
     # the reference's kernel shapes (one thread per item, its median-split tree, NEE inline), per
     # round on a 20-round sample of each scene: a secondary, extrapolated comparison
     t_ref_shape = sum(r * R.time_plain(s, 20, reference_shaped=True) for s, r in zip(specs, r_eff))
-    return {"target_rmse": TTR_TARGET, "workload": "batch of 16 uneven scenes, 256^2..1024^2, 2^16..2^21 photons",
+    return {"metric": "time to RMSE 0.01 (s), graph + batched vs plain", "target_rmse": TTR_TARGET,
+            "workload": "batch16: 16 uneven scenes, 256^2..1024^2 px, 2^16..2^21 photons, alpha U[0.6, 0.8]",
             "reference": f"fp32 GPU render, {TTR_REF_ROUNDS} rounds, independent seed", "reference_s": round(t_refs, 1),
+            "reference_vs_independent_check_rmse": [round(x, 5) for x in ref_vs_check],
+            "reference_noise_estimate": [round(x / 5 ** 0.5, 5) for x in ref_vs_check],
             "calibration": cal, "scenes": len(specs), "check_every": TTR_CHECK, "round_cap": TTR_MAX_ROUNDS,
             "rounds_to_target": r_star, "capped_scenes": capped,
-            "rmse_at_cap_or_target": [round(row, 5) for row in curve[-1][1]] if curve else None,
+            "rmse_at_last_check": [round(x, 5) for x in curve[-1][1]] if curve else None,
             "plain_final_rmse": [round(x, 5) for x in plain_rmse],
             "plain_s": round(t_plain, 3), "plain_s_per_scene": [round(dt, 3) for dt, _ in plain],
             "graph_batched_s": round(t_batch, 3), "speedup": round(t_plain / t_batch, 3),
             "plain_reference_shaped_s_extrapolated": round(t_ref_shape, 2),
             "speedup_vs_reference_shaped": round(t_ref_shape / t_batch, 2)}
+
+
+def time_to_rmse_small(a) -> dict | None:
+    """The small-scene study (16 uneven scenes of 32..64 px, 2^14..2^16 photons, converged FP64
+    oracle references committed in tests/golden/rmse_refs.npz): rounds to RMSE <= 0.01, and the
+    wall time of the graph + batched form (scenes retired at their own round counts) against the
+    plain per-pass form, scenes one at a time, timed per round on 40 rounds."""
+    import numpy as np
+
+    from phosphor_b200 import rmse as R
+    fx = ROOT / "tests" / "golden" / "rmse_refs.npz"
+    if not fx.exists():
+        return None
+    z = np.load(fx)
+    specs = R.rmse_batch()
+    refs = [z[f"scene{i}"].astype(np.float64) / 65535.0 for i in range(len(specs))]
+    max_rounds = 4096
+    r_star, curve = R.rounds_to_target(specs, refs, 0.01, max_rounds=max_rounds, check_every=4)
+    # a scene that has not reached the target by the cap is charged the cap in both forms
+    capped = [i for i, r in enumerate(r_star) if r is None]
+    r_eff = [max_rounds if r is None else r for r in r_star]
+    t_plain = [R.time_plain(s, 40) for s in specs]
+    t_ref = [R.time_plain(s, 40, reference_shaped=True) for s in specs]
+    t_batch = R.time_batched(specs, 200)
+    t_sched = R.time_batched_schedule(specs, r_eff)
+    out = {"target_rmse": 0.01, "reference": f"FP64 oracle, {int(z['rounds'])} rounds, independent seed",
+           "scenes": len(specs), "rounds_to_target": r_star, "round_cap": max_rounds, "capped_scenes": capped,
+           "final_rmse": [round(x, 5) for x in curve[-1][1]]}
+    tp = sum(r * t for r, t in zip(r_eff, t_plain))
+    tb = t_sched  # wall time, each scene retired from the batch at its own round count
+    tr = sum(r * t for r, t in zip(r_eff, t_ref))
+    out.update({"plain_s": round(tp, 3), "graph_batched_s": round(tb, 3), "speedup": round(tp / tb, 2),
+                "plain_reference_shaped_s": round(tr, 3), "speedup_vs_reference_shaped": round(tr / tb, 2),
+                "plain_ms_per_round": [round(1e3 * t, 3) for t in t_plain],
+                "plain_reference_shaped_ms_per_round": [round(1e3 * t, 3) for t in t_ref],
+                "batched_ms_per_round": round(1e3 * t_batch, 3),
+                "graph_batched_no_retire_s": round(max(r_eff) * t_batch, 3)})
+    return out
 
 
 def run_shard(a, cfg: dict) -> dict | None:
@@ -556,7 +607,7 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=list(CONFIGS) + ["batch16", "inverse"], default="caustic")
+    ap.add_argument("--config", choices=list(CONFIGS) + ["batch16", "inverse", "ttr16"], default="caustic")
     ap.add_argument("--no-rmse", action="store_true", help="skip the time-to-RMSE study (1 GPU only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-inverse", action="store_true", help="skip the inverse-rendering block (1 GPU only)")
@@ -582,6 +633,13 @@ def main() -> int:
             return 0
         print(json.dumps(run_batch16(a)))
         return 0
+    if a.config == "ttr16":
+        if a.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the time-to-RMSE study compares two forms of "
+                              "this library; use --config caustic"}))
+            return 0
+        print(json.dumps(time_to_rmse_batch16(a)))
+        return 0
     if a.config == "inverse":
         if a.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no adjoint; use --config"
@@ -602,7 +660,7 @@ def main() -> int:
     out = run_shard(a, cfg) if a.shard else run_ours(a, cfg)
     if out is not None:
         if not a.no_rmse and out["n_gpus"] == 1 and a.scale == 1:
-            out["time_to_rmse"] = time_to_rmse(a)
+            out["time_to_rmse"] = time_to_rmse_small(a)
         if not a.no_inverse and out["n_gpus"] == 1 and a.scale == 1:
             # inverse rendering through the adjoint (atrium 512x512, 200 Adam steps)
             inv = run_inverse(a)
