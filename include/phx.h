@@ -163,6 +163,9 @@ typedef struct phx_params {
 #define PHX_F_SIMPLE_TRAVERSAL 1u /* one-thread-per-ray kernels instead of the persistent ones */
 #define PHX_F_REFERENCE_BVH 2u    /* traverse the reference's median-split tree instead of the SAH tree */
 #define PHX_F_BINARY_BVH 4u       /* traverse the SAH tree as child pairs instead of 4-wide nodes */
+#define PHX_F_DEVICE_BVH 8u       /* build the SAH traversal tree on the GPU (the same tree, bit for
+                                     bit; the reference tree for tie-break ranks is built on the host
+                                     meanwhile) */
 
 /* Counters and sizes of a context. */
 typedef struct phx_info {
@@ -185,7 +188,9 @@ typedef struct phx_info {
     uint32_t trav_depth;          /* depth of the device traversal tree */
     uint32_t trav_inner_nodes;    /* inner (child-pair) nodes of the device traversal tree */
     uint32_t spec_samples;        /* specular-NEE shadow rays the last camera pass deferred (all scenes) */
-    uint32_t reserved[3];
+    float setup_ms;               /* wall time of this scene's setup (trees, uploads) */
+    float bvh_build_ms;           /* of which: building the reference and traversal trees */
+    uint32_t reserved[1];
 } phx_info;
 
 /* Buffers readable / writable through phx_read_buffer / phx_write_buffer, always in the
@@ -268,6 +273,28 @@ PHX_API int phx_image(void *ctx, float exposure, int tonemap, uint64_t total_pho
 /* Host-side helpers (no GPU needed). */
 /* Bvh::Bvh (src/renderer/bvh.cpp:74-84): writes 2n-1 nodes; returns the tree depth in *depth. */
 PHX_API int phx_bvh_build(const phx_triangle *tris, uint32_t n, phx_bvh_node *out_nodes, uint32_t *depth);
+/* The traversal tree the kernels walk (no reference counterpart: the reference traverses the tree of
+ * bvh.cpp): a binned-SAH tree over the reference's expanded triangle boxes with leaves of up to
+ * max_leaf (1..16) triangles, as child pairs (16 floats per inner node) or collapsed to 4-wide
+ * nodes (28 floats), each triangle record (12 floats, leaf order) carrying its leaf rank in the
+ * reference tree.  device < 0 builds on the host; device >= 0 builds on that GPU (PHX_F_DEVICE_BVH)
+ * and returns the same arrays bit for bit.  nodes needs room for 16 (or 28) floats per triangle,
+ * trirec 12 floats and leaf_tri one entry per triangle.  build_ms: wall time of the traversal tree
+ * (for the GPU: its build with the triangles resident on the device and the records written there),
+ * excluding the reference tree that supplies the ranks. */
+typedef struct phx_bvh_packed {
+    float *nodes;
+    float *trirec;
+    uint32_t *leaf_tri;
+    uint32_t n_nodes;  /* out: inner (child-pair or 4-wide) nodes */
+    int32_t root;      /* out: root reference (>= 0 inner node, < 0 leaf ~(first | (count-1) << 27)) */
+    uint32_t depth;    /* out: depth of the child-pair tree */
+    uint32_t wdepth;   /* out: depth of the 4-wide tree (0 for child pairs) */
+    float build_ms;    /* out */
+    uint32_t reserved[3];
+} phx_bvh_packed;
+PHX_API int phx_traversal_bvh_build(const phx_triangle *tris, uint32_t n, uint32_t max_leaf, int wide, int device,
+                                    phx_bvh_packed *out);
 /* build_photon_hash_info (include/common/photon_hash.h:41-50) from the BVH root box. */
 PHX_API int phx_hash_info(const phx_bvh_node *root, uint32_t grid_res, phx_photon_hash_data *out);
 /* Camera::Camera + Camera::focus + Camera::to_params (src/renderer/camera.cpp:3-56). */

@@ -24,7 +24,7 @@ STATUS_NAMES = {0: "PHX_OK", 1: "PHX_E_INVALID", 2: "PHX_E_OOM", 3: "PHX_E_CUDA"
 PHX_NO_TEXTURE = 0xFFFFFFFF
 PHX_LIGHT_POINT, PHX_LIGHT_SPOT, PHX_LIGHT_DIRECTIONAL, PHX_LIGHT_TEXTURED = range(4)
 PHX_SCENE_CORNELL, PHX_SCENE_CAUSTIC, PHX_SCENE_ATRIUM = range(3)
-PHX_F_DEFAULT, PHX_F_SIMPLE_TRAVERSAL, PHX_F_REFERENCE_BVH, PHX_F_BINARY_BVH = 0, 1, 2, 4
+PHX_F_DEFAULT, PHX_F_SIMPLE_TRAVERSAL, PHX_F_REFERENCE_BVH, PHX_F_BINARY_BVH, PHX_F_DEVICE_BVH = 0, 1, 2, 4, 8
 
 BUFFERS = ["HP_POS", "HP_NORMAL", "HP_THROUGHPUT", "HP_BASE_COLOR", "HP_DIRECT", "HP_EMISSION", "FLUX",
            "PHOTON_WEIGHT", "RADIANCE", "PHOTON_POS", "PHOTON_POWER", "PHOTON_DIR", "PHOTON_HASH", "CELL_COUNT",
@@ -119,7 +119,8 @@ class Info(C.Structure):
                [("total_photons_emitted", C.c_uint64), ("stack_overflows", C.c_uint32), ("error_flags", C.c_uint32),
                 ("_pad0", C.c_uint32 * 2), ("hash", PhotonHashData), ("kernels_per_round", C.c_uint32),
                 ("sort_passes", C.c_uint32), ("trav_depth", C.c_uint32), ("trav_inner_nodes", C.c_uint32),
-                ("spec_samples", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("spec_samples", C.c_uint32), ("setup_ms", C.c_float), ("bvh_build_ms", C.c_float),
+                ("reserved", C.c_uint32 * 1)]
 
 
 class GltfOptions(C.Structure):
@@ -139,8 +140,15 @@ class Tuning(C.Structure):
                [("reserved", C.c_uint32 * 1)]
 
 
+class BvhPacked(C.Structure):
+    _fields_ = [("nodes", C.POINTER(C.c_float)), ("trirec", C.POINTER(C.c_float)),
+                ("leaf_tri", C.POINTER(C.c_uint32)), ("n_nodes", C.c_uint32), ("root", C.c_int32),
+                ("depth", C.c_uint32), ("wdepth", C.c_uint32), ("build_ms", C.c_float),
+                ("reserved", C.c_uint32 * 3)]
+
+
 SIZES = {Triangle: 176, Material: 96, UvTransformBlock: 192, Light: 128, CameraParams: 112, BvhNode: 32,
-         PhotonHashData: 48, TextureMeta: 16, Scene: 240, Info: 144, Params: 64, Tuning: 48, SceneSpec: 40}
+         PhotonHashData: 48, TextureMeta: 16, Scene: 240, Info: 144, Params: 64, Tuning: 48, SceneSpec: 40, BvhPacked: 56}
 
 # (name, restype, argtypes) of every entry point declared in include/phx.h
 VP = C.c_void_p
@@ -161,6 +169,8 @@ PROTOTYPES = [
     ("phx_set_n_photons", C.c_int, [VP, C.c_uint32]),
     ("phx_image", C.c_int, [VP, C.c_float, C.c_int, C.c_uint64, C.c_uint32, VP, VP]),
     ("phx_bvh_build", C.c_int, [C.POINTER(Triangle), C.c_uint32, C.POINTER(BvhNode), C.POINTER(C.c_uint32)]),
+    ("phx_traversal_bvh_build", C.c_int, [C.POINTER(Triangle), C.c_uint32, C.c_uint32, C.c_int, C.c_int,
+                                          C.POINTER(BvhPacked)]),
     ("phx_hash_info", C.c_int, [C.POINTER(BvhNode), C.c_uint32, C.POINTER(PhotonHashData)]),
     ("phx_camera_make", C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float,
                                   C.c_float, C.c_float, C.c_float, C.POINTER(CameraParams)]),

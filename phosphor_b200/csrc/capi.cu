@@ -4,6 +4,7 @@
 #include "engine.hpp"
 #include "nccl_dl.hpp"
 
+#include <chrono>
 #include <cstring>
 #include <new>
 
@@ -187,6 +188,96 @@ PHX_API int phx_bvh_build(const phx_triangle *tris, uint32_t n, phx_bvh_node *ou
         if (!bvh_build(tris, n, nodes, depth))
             return fail(PHX_E_INVALID, "degenerate or infinite triangle bounding box");
         std::memcpy(out, nodes.data(), nodes.size() * sizeof(phx_bvh_node));
+        return PHX_OK;
+    });
+}
+
+#ifndef CK
+#define CK(x)                                                                                                          \
+    do {                                                                                                               \
+        cudaError_t e_ = (x);                                                                                          \
+        if (e_ != cudaSuccess)                                                                                         \
+            return fail(PHX_E_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));                                  \
+    } while (0)
+#endif
+
+PHX_API int phx_traversal_bvh_build(const phx_triangle *tris, uint32_t n, uint32_t max_leaf, int wide, int device,
+                                    phx_bvh_packed *out) {
+    return guard([&]() -> int {
+        if (!tris || !out || !out->nodes || !out->trirec || !out->leaf_tri || n == 0 || max_leaf < 1 || max_leaf > 16)
+            return fail(PHX_E_INVALID, "bad arguments");
+        std::vector<phx_bvh_node> ref;
+        if (!bvh_build(tris, n, ref, nullptr))
+            return fail(PHX_E_INVALID, "degenerate or infinite triangle bounding box");
+        const std::vector<uint32_t> ranks = reference_leaf_ranks(ref, n);
+        const uint32_t per = wide ? 28u : 16u;
+        if (device < 0) {
+            const auto t0 = std::chrono::steady_clock::now();
+            PackedBvh pk;
+            if (!bvh_build_sah(tris, n, ranks, max_leaf, pk))
+                return fail(PHX_E_INVALID, "SAH build failed");
+            if (wide)
+                bvh_widen(pk);
+            out->build_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            const std::vector<float> &nodes = wide ? pk.wnodes : pk.cnodes;
+            std::memcpy(out->nodes, nodes.data(), nodes.size() * 4);
+            std::memcpy(out->trirec, pk.trirec.data(), pk.trirec.size() * 4);
+            std::memcpy(out->leaf_tri, pk.leaf_tri.data(), pk.leaf_tri.size() * 4);
+            out->n_nodes = (uint32_t)(nodes.size() / per);
+            out->root = wide ? pk.wroot : pk.root;
+            out->depth = pk.depth;
+            out->wdepth = wide ? pk.wdepth : 0u;
+            return PHX_OK;
+        }
+        CK(cudaSetDevice(device));
+        cudaStream_t st;
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        struct Cleanup {
+            cudaStream_t st;
+            std::vector<void *> p;
+            DeviceBvh db;
+            ~Cleanup() {
+                db.release();
+                for (void *q : p)
+                    cudaFree(q);
+                cudaStreamDestroy(st);
+            }
+        } c{st, {}, {}};
+        auto dalloc = [&](size_t bytes) -> void * {
+            void *q = nullptr;
+            if (cudaMalloc(&q, std::max<size_t>(bytes, 16)) != cudaSuccess)
+                return nullptr;
+            c.p.push_back(q);
+            return q;
+        };
+        auto *d_tris = static_cast<phx_triangle *>(dalloc(sizeof(phx_triangle) * (size_t)n));
+        auto *d_rank = static_cast<uint32_t *>(dalloc(4 * (size_t)n));
+        auto *d_rec = static_cast<float4 *>(dalloc(48 * (size_t)n));
+        auto *d_nrm = static_cast<float4 *>(dalloc(48 * (size_t)n));
+        auto *d_tan = static_cast<float4 *>(dalloc(48 * (size_t)n));
+        auto *d_uv = static_cast<float4 *>(dalloc(32 * (size_t)n));
+        if (!d_tris || !d_rank || !d_rec || !d_nrm || !d_tan || !d_uv)
+            return fail(PHX_E_OOM, "device allocation failed");
+        CK(cudaMemcpy(d_tris, tris, sizeof(phx_triangle) * (size_t)n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_rank, ranks.data(), 4 * (size_t)n, cudaMemcpyHostToDevice));
+        const auto t0 = std::chrono::steady_clock::now();
+        std::string msg;
+        const int rc = bvh_device_build(d_tris, n, max_leaf, wide != 0, st, c.db, msg);
+        if (rc)
+            return fail(rc == 2 ? PHX_E_OOM : rc == 1 ? PHX_E_INVALID : PHX_E_CUDA, msg);
+        if (bvh_device_finish(d_tris, d_rank, n, c.db, d_rec, d_nrm, d_tan, d_uv, st))
+            return fail(PHX_E_CUDA, "device BVH triangle records: launch failed");
+        CK(cudaStreamSynchronize(st));
+        out->build_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        out->n_nodes = wide ? c.db.n_wide : c.db.n_inner;
+        out->root = wide ? c.db.wroot : c.db.root;
+        out->depth = c.db.depth;
+        out->wdepth = wide ? c.db.wdepth : 0u;
+        if (out->n_nodes)
+            CK(cudaMemcpy(out->nodes, wide ? c.db.wnodes : c.db.cnodes, (size_t)out->n_nodes * per * 4,
+                          cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(out->trirec, d_rec, 48 * (size_t)n, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(out->leaf_tri, c.db.leaf_tri, 4 * (size_t)n, cudaMemcpyDeviceToHost));
         return PHX_OK;
     });
 }

@@ -6,6 +6,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <chrono>
+#include <thread>
 
 namespace phx {
 
@@ -145,10 +147,72 @@ uint32_t light_sample_draws(const phx_light *l, uint32_t n, float total_lum) {
     return draws;
 }
 
+static float ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// The SAH traversal tree built on the device (k_bvh.cu) while a host thread builds the reference
+// tree, whose leaf ranks only the last step needs.  done = false: the caller builds on the host
+// (force_ref: the SAH tree is too deep for the traversal stack, use the reference tree).
+static int device_traversal(SceneSlot &S, const phx_scene &s, const phx_params &p, cudaStream_t st, bool &ref_built,
+                            bool &done, bool &force_ref, int32_t &root, bool &wide) {
+    const uint32_t n = s.n_triangles;
+    DevBuf tris, rank;
+    int r;
+    if ((r = upload(tris, s.triangles, sizeof(phx_triangle) * (size_t)n)))
+        return r;
+    bool ref_ok = false;
+    std::vector<uint32_t> ranks;
+    std::thread ref([&] {
+        ref_ok = bvh_build(s.triangles, n, S.nodes, &S.depth);
+        if (ref_ok)
+            ranks = reference_leaf_ranks(S.nodes, n);
+    });
+    DeviceBvh db;
+    std::string msg;
+    const bool want_wide = !(p.flags & PHX_F_BINARY_BVH);
+    const int rc =
+        bvh_device_build(tris.as<phx_triangle>(), n, p.bvh_leaf_size ? p.bvh_leaf_size : 4u, want_wide, st, db, msg);
+    ref.join();
+    ref_built = ref_ok;
+    struct Release {
+        DeviceBvh &b;
+        ~Release() { b.release(); }
+    } release{db};
+    if (!ref_ok)
+        return fail(PHX_E_INVALID, "degenerate or infinite triangle bounding box (bounding_box.h:17-28)");
+    if (rc)
+        return fail(rc == 2 ? PHX_E_OOM : rc == 1 ? PHX_E_INVALID : PHX_E_CUDA, msg);
+    if (!(db.depth + 2 < (uint32_t)TRAV_STACK)) {
+        force_ref = true;
+        return PHX_OK;
+    }
+    wide = want_wide && 3 * db.wdepth + 4 < (uint32_t)TRAV_STACK;
+    const float *nodes = wide ? db.wnodes : db.cnodes;
+    const uint32_t n_nodes = wide ? db.n_wide : db.n_inner, per = wide ? 28u : 16u;
+    S.trav_depth = wide ? db.wdepth : db.depth;
+    S.trav_inner = n_nodes;
+    root = wide ? db.wroot : db.root;
+    if ((r = upload(S.bufs[0], nullptr, std::max<size_t>((size_t)n_nodes * per, 4) * 4)) ||
+        (r = S.bufs[1].alloc((size_t)n * 48)) || (r = S.bufs[2].alloc((size_t)n * 48)) ||
+        (r = S.bufs[3].alloc((size_t)n * 48)) || (r = S.bufs[4].alloc((size_t)n * 32)) ||
+        (r = upload(rank, ranks.data(), 4 * (size_t)n)))
+        return r;
+    if (n_nodes)
+        CK(cudaMemcpyAsync(S.bufs[0].p, nodes, (size_t)n_nodes * per * 4, cudaMemcpyDeviceToDevice, st));
+    if (bvh_device_finish(tris.as<phx_triangle>(), rank.as<u32>(), n, db, S.bufs[1].as<float4>(),
+                          S.bufs[2].as<float4>(), S.bufs[3].as<float4>(), S.bufs[4].as<float4>(), st))
+        return fail(PHX_E_CUDA, "device BVH triangle records: launch failed");
+    CK(cudaStreamSynchronize(st));
+    done = true;
+    return PHX_OK;
+}
+
 int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, uint32_t *pix, uint32_t *emit,
                          uint32_t *cell, uint64_t *slot) {
     SceneSlot &S = sc[i];
     S.prm = p;
+    const auto t_setup = std::chrono::steady_clock::now();
     if (!s.triangles || s.n_triangles == 0)
         return fail(PHX_E_INVALID, "scene has no triangles");
     if (!s.materials || s.n_materials == 0)
@@ -184,42 +248,58 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
             if (k != PHX_NO_TEXTURE && k >= s.n_textures)
                 return fail(PHX_E_INVALID, "material texture index out of range");
     }
-    if (!bvh_build(s.triangles, s.n_triangles, S.nodes, &S.depth))
-        return fail(PHX_E_INVALID, "degenerate or infinite triangle bounding box (bounding_box.h:17-28)");
-    // Traversal tree: binned SAH over the same expanded boxes (fewer node visits), or the
-    // reference tree itself.  Either returns the reference's hit for every ray: the closest t,
-    // ties broken by the reference leaf rank carried in each triangle record.
-    PackedBvh pk;
-    bool sah = !(p.flags & PHX_F_REFERENCE_BVH);
-    if (sah) {
-        std::vector<uint32_t> ranks = reference_leaf_ranks(S.nodes, s.n_triangles);
-        sah = bvh_build_sah(s.triangles, s.n_triangles, ranks, p.bvh_leaf_size ? p.bvh_leaf_size : 4u, pk) &&
-              pk.depth + 2 < (uint32_t)TRAV_STACK;
-    }
-    if (!sah)
-        bvh_pack(S.nodes, s.triangles, pk);
-    // 4-wide nodes over the SAH tree (half the dependent node fetches per ray) unless asked for the
-    // binary form or the worst-case stack (3 pushes per level) could exceed the traversal stack
-    bool wide = false;
-    if (sah && !(p.flags & PHX_F_BINARY_BVH)) {
-        bvh_widen(pk);
-        wide = 3 * pk.wdepth + 4 < (uint32_t)TRAV_STACK;
-    }
-    S.trav_depth = wide ? pk.wdepth : sah ? pk.depth : S.depth;
-    S.trav_inner = wide ? (uint32_t)(pk.wnodes.size() / 28) : (uint32_t)(pk.cnodes.size() / 16);
     const uint32_t n = s.n_triangles;
     S.n_tris = n;
-    std::vector<float> nrm((size_t)n * 12), tan((size_t)n * 12), uv((size_t)n * 8);
-    for (uint32_t r = 0; r < n; r++) {
-        const phx_triangle &t = s.triangles[pk.leaf_tri[r]];
-        const phx_f4 *nn[3] = {&t.n0, &t.n1, &t.n2}, *tt[3] = {&t.t0, &t.t1, &t.t2};
-        for (int k = 0; k < 3; k++) {
-            std::memcpy(&nrm[(size_t)r * 12 + 4 * k], nn[k], 16);
-            std::memcpy(&tan[(size_t)r * 12 + 4 * k], tt[k], 16);
+    S.bufs.resize(16);
+    int r;
+    int32_t trav_root = 0;
+    bool wide = false, trav_done = false, ref_built = false, force_ref = false;
+    if ((p.flags & PHX_F_DEVICE_BVH) && !(p.flags & PHX_F_REFERENCE_BVH) &&
+        (r = device_traversal(S, s, p, st, ref_built, trav_done, force_ref, trav_root, wide)))
+        return r;
+    if (!trav_done) {
+        if (!ref_built && !bvh_build(s.triangles, s.n_triangles, S.nodes, &S.depth))
+            return fail(PHX_E_INVALID, "degenerate or infinite triangle bounding box (bounding_box.h:17-28)");
+        // Traversal tree: binned SAH over the same expanded boxes (fewer node visits), or the
+        // reference tree itself.  Either returns the reference's hit for every ray: the closest t,
+        // ties broken by the reference leaf rank carried in each triangle record.
+        PackedBvh pk;
+        bool sah = !(p.flags & PHX_F_REFERENCE_BVH) && !force_ref;
+        if (sah) {
+            std::vector<uint32_t> ranks = reference_leaf_ranks(S.nodes, s.n_triangles);
+            sah = bvh_build_sah(s.triangles, s.n_triangles, ranks, p.bvh_leaf_size ? p.bvh_leaf_size : 4u, pk) &&
+                  pk.depth + 2 < (uint32_t)TRAV_STACK;
         }
-        float u8v[8] = {t.uv0.x, t.uv0.y, t.uv1.x, t.uv1.y, t.uv2.x, t.uv2.y, 0.0f, 0.0f};
-        std::memcpy(&uv[(size_t)r * 8], u8v, 32);
+        if (!sah)
+            bvh_pack(S.nodes, s.triangles, pk);
+        // 4-wide nodes over the SAH tree (half the dependent node fetches per ray) unless asked for
+        // the binary form or the worst-case stack (3 pushes per level) could exceed the traversal stack
+        if (sah && !(p.flags & PHX_F_BINARY_BVH)) {
+            bvh_widen(pk);
+            wide = 3 * pk.wdepth + 4 < (uint32_t)TRAV_STACK;
+        }
+        S.trav_depth = wide ? pk.wdepth : sah ? pk.depth : S.depth;
+        S.trav_inner = wide ? (uint32_t)(pk.wnodes.size() / 28) : (uint32_t)(pk.cnodes.size() / 16);
+        trav_root = wide ? pk.wroot : pk.root;
+        std::vector<float> nrm((size_t)n * 12), tan((size_t)n * 12), uv((size_t)n * 8);
+        for (uint32_t k = 0; k < n; k++) {
+            const phx_triangle &t = s.triangles[pk.leaf_tri[k]];
+            const phx_f4 *nn[3] = {&t.n0, &t.n1, &t.n2}, *tt[3] = {&t.t0, &t.t1, &t.t2};
+            for (int j = 0; j < 3; j++) {
+                std::memcpy(&nrm[(size_t)k * 12 + 4 * j], nn[j], 16);
+                std::memcpy(&tan[(size_t)k * 12 + 4 * j], tt[j], 16);
+            }
+            float u8v[8] = {t.uv0.x, t.uv0.y, t.uv1.x, t.uv1.y, t.uv2.x, t.uv2.y, 0.0f, 0.0f};
+            std::memcpy(&uv[(size_t)k * 8], u8v, 32);
+        }
+        const std::vector<float> &inner = wide ? pk.wnodes : pk.cnodes;
+        if ((r = upload(S.bufs[0], inner.data(), std::max<size_t>(inner.size(), 4) * 4)) ||
+            (r = upload(S.bufs[1], pk.trirec.data(), pk.trirec.size() * 4)) ||
+            (r = upload(S.bufs[2], nrm.data(), nrm.size() * 4)) ||
+            (r = upload(S.bufs[3], tan.data(), tan.size() * 4)) || (r = upload(S.bufs[4], uv.data(), uv.size() * 4)))
+            return r;
     }
+    S.bvh_ms = ms_since(t_setup);
     const uint32_t ne = s.n_emissive_triangles;
     std::vector<float> ev((size_t)std::max(ne, 1u) * 12, 0.0f), en((size_t)std::max(ne, 1u) * 12, 0.0f),
         euv((size_t)std::max(ne, 1u) * 8, 0.0f);
@@ -251,13 +331,7 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
         else
             lum_pref_sum(s.lights, s.n_lights, lum.data());
     }
-    S.bufs.resize(16);
-    int r;
-    const std::vector<float> &inner = wide ? pk.wnodes : pk.cnodes;
-    if ((r = upload(S.bufs[0], inner.data(), std::max<size_t>(inner.size(), 4) * 4)) ||
-        (r = upload(S.bufs[1], pk.trirec.data(), pk.trirec.size() * 4)) ||
-        (r = upload(S.bufs[2], nrm.data(), nrm.size() * 4)) || (r = upload(S.bufs[3], tan.data(), tan.size() * 4)) ||
-        (r = upload(S.bufs[4], uv.data(), uv.size() * 4)) || (r = upload(S.bufs[5], ev.data(), ev.size() * 4)) ||
+    if ((r = upload(S.bufs[5], ev.data(), ev.size() * 4)) ||
         (r = upload(S.bufs[6], en.data(), en.size() * 4)) || (r = upload(S.bufs[7], euv.data(), euv.size() * 4)) ||
         (r = upload(S.bufs[8], emat.data(), emat.size() * 4)) ||
         (r = upload(S.bufs[9], s.materials, sizeof(phx_material) * s.n_materials)) ||
@@ -292,7 +366,7 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
     d.lights = S.bufs[13].as<phx_light>();
     d.lum_pref_sum = S.bufs[14].as<float>();
     d.envmap = S.bufs[15].as<float>();
-    d.root = wide ? pk.wroot : pk.root;
+    d.root = trav_root;
     d.wide = wide ? 1u : 0u;
     d.n_tris = n;
     d.n_lights = s.n_lights;
@@ -339,6 +413,7 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
     *emit += d.n_emit;
     *cell += d.n_cells;
     *slot += (uint64_t)d.n_emit * d.max_bounces;
+    S.setup_ms = ms_since(t_setup);
     return PHX_OK;
 }
 
@@ -1447,6 +1522,8 @@ int Engine::info(uint32_t s, phx_info *o) {
     o->sort_passes = radix_passes(key_bits);
     o->trav_depth = S.trav_depth;
     o->trav_inner_nodes = S.trav_inner;
+    o->setup_ms = S.setup_ms;
+    o->bvh_build_ms = S.bvh_ms;
     // seeds, trace, [sample, shadow, resolve], emit, count scan, compaction, hash, cell scan, 3 per
     // sort pass, records, gather (+1 with the specular NEE deferred: its resolve; k_shadow traces
     // its rays).  The sampling kernel runs only for scenes whose light samples vary in RNG draws.

@@ -34,6 +34,7 @@ struct SceneSlot {
     std::vector<phx_bvh_node> nodes; // the reference tree (read-back, grid box, tie-break ranks)
     uint32_t depth = 0;
     uint32_t trav_depth = 0, trav_inner = 0; // the device traversal tree
+    float setup_ms = 0.0f, bvh_ms = 0.0f;     // wall time of the scene setup, of which the trees
     uint32_t n_tris = 0;
     std::vector<DevBuf> bufs;
     SceneDesc desc{};

@@ -375,7 +375,9 @@ bool bvh_build_sah(const phx_triangle *tris, uint32_t n, const std::vector<uint3
         uint32_t mid;
         if (bax >= 0) {
             const float ext = chi[bax] - clo[bax], sc = nb / ext;
-            auto it = std::partition(P.begin() + b, P.begin() + e, [&](const Prim &p) {
+            // stable: every range keeps ascending triangle order, so the object-median fallback
+            // below splits a defined sequence (the device builder makes the same tree)
+            auto it = std::stable_partition(P.begin() + b, P.begin() + e, [&](const Prim &p) {
                 return std::min(nb - 1, (int)((p.c[bax] - clo[bax]) * sc)) < bbin;
             });
             mid = (uint32_t)(it - P.begin());

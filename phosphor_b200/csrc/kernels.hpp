@@ -109,6 +109,26 @@ int scan_noalloc(const u32 *in, u32 *out, u32 n, u32 *total, cudaStream_t st, st
 int denoise_filter(int mode, const int32_t *in, float *out, const float *weights, uint32_t width, uint32_t height,
                    uint32_t k, float *kernel_ms, std::string &msg);
 
+// k_bvh.cu: the binned-SAH traversal tree built on the device, identical to the host builder's
+// (bvh_build_sah, then bvh_widen when `widen`).  Topology first; bvh_device_finish then orders each
+// leaf by reference rank and writes the per-triangle records (trirec 3, nrm 3, tan 3, uv 2 float4
+// per triangle, leaf order).  Returns 0 ok, 1 invalid input, 2 out of memory, 3 CUDA error.
+struct DeviceBvh {
+    float *cnodes = nullptr; // 16 floats per inner node, pre-order (max(n_inner, 1) records)
+    float *wnodes = nullptr; // 28 floats per 4-wide node, pre-order (when widened)
+    u32 *leaf_tri = nullptr; // triangle index per leaf position
+    uint2 *leaves = nullptr; // (first, count) per leaf
+    u32 n_inner = 0, depth = 0, n_leaves = 0, levels = 0;
+    int root = 0;            // 0 or a leaf reference
+    u32 n_wide = 0, wdepth = 0;
+    int wroot = 0;
+    void release();
+};
+int bvh_device_build(const phx_triangle *tris, u32 n, u32 max_leaf, bool widen, cudaStream_t st, DeviceBvh &out,
+                     std::string &err);
+int bvh_device_finish(const phx_triangle *tris, const u32 *rank, u32 n, DeviceBvh &b, float4 *trirec, float4 *nrm,
+                      float4 *tan, float4 *uv, cudaStream_t st);
+
 // stable LSD radix sort of (key, canonical index) by key; n read from device *n_dev (<= n_max)
 size_t radix_scratch_bytes(u64 n_max, u32 key_bits);
 u32 radix_passes(u32 key_bits);

@@ -163,6 +163,33 @@ def bvh_build(scene: SceneData) -> tuple[np.ndarray, int]:
     return np.frombuffer(bytes(out), dtype=np.float32).reshape(2 * n - 1, 8).copy(), depth.value
 
 
+@dataclasses.dataclass
+class TraversalBvh:
+    nodes: np.ndarray      # (n_nodes, 16) child pairs or (n_nodes, 28) 4-wide, float32 (refs as int32 bits)
+    trirec: np.ndarray     # (n, 12) float32, leaf order
+    leaf_tri: np.ndarray   # (n,) uint32
+    root: int
+    depth: int
+    wdepth: int
+    build_ms: float
+
+
+def traversal_bvh(scene: SceneData, max_leaf: int = 4, wide: bool = True, device: int = -1) -> TraversalBvh:
+    """The SAH traversal tree the kernels walk, built on the host (device < 0) or on a GPU."""
+    lib = A.load()
+    n = scene.scene.n_triangles
+    per = 28 if wide else 16
+    nodes = np.zeros((max(n, 1), per), np.float32)
+    trirec = np.zeros((n, 12), np.float32)
+    leaf = np.zeros(n, np.uint32)
+    out = A.BvhPacked()
+    out.nodes = nodes.ctypes.data_as(C.POINTER(C.c_float))
+    out.trirec = trirec.ctypes.data_as(C.POINTER(C.c_float))
+    out.leaf_tri = leaf.ctypes.data_as(C.POINTER(C.c_uint32))
+    A.check(lib.phx_traversal_bvh_build(scene.scene.triangles, n, max_leaf, int(wide), device, C.byref(out)))
+    return TraversalBvh(nodes[:out.n_nodes].copy(), trirec, leaf, out.root, out.depth, out.wdepth, out.build_ms)
+
+
 def camera_make(position, look_at, up, hfov_deg, aspect, defocus_angle=0.0, focus_distance=1.0) -> A.CameraParams:
     lib = A.load()
     f3 = C.c_float * 3

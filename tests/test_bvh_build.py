@@ -1,0 +1,239 @@
+"""The traversal tree: the host builder's tree is valid (CPU), and the GPU builder returns the same
+arrays bit for bit and renders the same images (PHX_F_DEVICE_BVH, needs a GPU).
+
+The SAH tree is the kernels' own structure (the reference traverses the median-split tree of
+src/renderer/bvh.cpp); what it must preserve is the reference's hit for every ray, which the
+tie-break rank carried in each triangle record guarantees for any tree over the same boxes.  Here
+the checks are structural: every triangle sits in exactly one leaf, every child box bounds its
+subtree, leaves keep the reference-rank order, and the device build equals the host build.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import phosphor_b200 as P
+from phosphor_b200 import _capi as A
+from phosphor_b200 import renderer as R
+
+LEAF_BITS = 27
+EMPTY = 0x7FFFFFFF
+
+
+def soup(verts: np.ndarray) -> P.SceneData:
+    """A scene of bare triangles (n, 3, 3) for the tree builders (no materials needed)."""
+    n = len(verts)
+    rec = np.zeros((n, 44), np.float32)
+    rec[:, 0:3], rec[:, 4:7], rec[:, 8:11] = verts[:, 0], verts[:, 1], verts[:, 2]
+    rec[:, 12:15] = rec[:, 16:19] = rec[:, 20:23] = (0.0, 0.0, 1.0)
+    sc = A.Scene()
+    sc.triangles = rec.ctypes.data_as(C.POINTER(A.Triangle))
+    sc.n_triangles = n
+    return P.SceneData(sc, keep=(rec,))
+
+
+def random_soup(n, seed=0, scale=10.0, size=0.3):
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(-scale, scale, (n, 1, 3))
+    return soup((c + rng.normal(0, size, (n, 3, 3))).astype(np.float32))
+
+
+def coincident_soup(n_same, n_other, seed=1):
+    """n_same copies of one triangle (every centroid equal: the object-median fallback) + others."""
+    rng = np.random.default_rng(seed)
+    same = np.repeat(np.array([[[0, 0, 0], [1, 0, 0], [0, 1, 0]]], np.float32), n_same, axis=0)
+    c = rng.uniform(-5, 5, (n_other, 1, 3))
+    other = (c + rng.normal(0, 0.2, (n_other, 3, 3))).astype(np.float32)
+    return soup(np.concatenate([same, other]).astype(np.float32))
+
+
+def grid_soup(side):
+    """A height-field-like sheet: rows of triangles whose centroids tie on two axes."""
+    xs, zs = np.meshgrid(np.arange(side, dtype=np.float32), np.arange(side, dtype=np.float32))
+    p00 = np.stack([xs, np.zeros_like(xs), zs], -1).reshape(-1, 3)
+    t1 = np.stack([p00, p00 + (1, 0, 0), p00 + (0, 0, 1)], 1)
+    t2 = np.stack([p00 + (1, 0, 0), p00 + (1, 0, 1), p00 + (0, 0, 1)], 1)
+    return soup(np.concatenate([t1, t2]).astype(np.float32))
+
+
+def ref_ranks(scene):
+    nodes, _ = R.bvh_build(scene)
+    tri = nodes[:, 3].view(np.uint32)
+    leaves = tri[tri != 0xFFFFFFFF]
+    rank = np.empty(scene.n_triangles, np.uint32)
+    rank[leaves] = np.arange(len(leaves), dtype=np.uint32)
+    return rank
+
+
+def expanded_boxes(scene):
+    v = scene.triangle_vertices().astype(np.float32)
+    return v.min(axis=1) - np.float32(1e-3), v.max(axis=1) + np.float32(1e-3)
+
+
+def check_tree(scene, b: R.TraversalBvh, wide: bool, max_leaf: int):
+    n = scene.n_triangles
+    lo_t, hi_t = expanded_boxes(scene)
+    rank = ref_ranks(scene)
+    seen = np.zeros(n, np.int32)
+    per = 28 if wide else 16
+    refs_at = (24, 28) if wide else (12, 14)
+
+    def children(node):
+        row = b.nodes[node]
+        refs = row[refs_at[0]:refs_at[1]].view(np.int32)
+        out = []
+        for k, r in enumerate(refs):
+            if wide and r == EMPTY:
+                continue
+            if wide:
+                lo = np.array([row[8 * a + k] for a in range(3)])
+                hi = np.array([row[8 * a + 4 + k] for a in range(3)])
+            else:
+                lo = np.array([row[4 * k], row[4 * k + 2], row[8 + 2 * k]])
+                hi = np.array([row[4 * k + 1], row[4 * k + 3], row[9 + 2 * k]])
+            out.append((int(r), lo, hi))
+        return out
+
+    def leaf_range(r):
+        enc = ~r & 0xFFFFFFFF
+        return enc & ((1 << LEAF_BITS) - 1), (enc >> LEAF_BITS) + 1
+
+    def visit_leaf(r, lo, hi):
+        first, cnt = leaf_range(r)
+        assert 1 <= cnt <= max_leaf
+        tris = b.leaf_tri[first:first + cnt]
+        seen[tris] += 1
+        assert np.all(np.diff(rank[tris].astype(np.int64)) > 0), "leaf not in reference-rank order"
+        if lo is not None:
+            assert np.all(lo_t[tris] >= lo) and np.all(hi_t[tris] <= hi), "leaf box does not bound its triangles"
+        assert np.array_equal(b.trirec[first:first + cnt, 7].view(np.uint32), rank[tris])
+
+    order = []
+    if b.root < 0:
+        visit_leaf(b.root, None, None)
+    else:
+        stack = [(b.root, None, None)]
+        while stack:
+            node, lo, hi = stack.pop()
+            order.append(node)
+            kids = children(node)
+            assert len(kids) >= 2
+            for r, clo, chi in kids:
+                if lo is not None:
+                    assert np.all(clo >= lo) and np.all(chi <= hi), "child box outside its parent's"
+            for r, clo, chi in reversed(kids):
+                if r >= 0:
+                    stack.append((r, clo, chi))
+                else:
+                    visit_leaf(r, clo, chi)
+        assert order == list(range(len(b.nodes))), "nodes are not numbered in pre-order"
+    assert np.all(seen == 1), "a triangle is missing from the leaves or repeated"
+    assert b.nodes.shape[1] == per
+
+
+@pytest.mark.parametrize("wide", [False, True])
+@pytest.mark.parametrize("max_leaf", [1, 4, 16])
+def test_host_tree_structure(wide, max_leaf):
+    for scene in (random_soup(3000, 2), coincident_soup(300, 200), grid_soup(24)):
+        b = R.traversal_bvh(scene, max_leaf, wide, -1)
+        check_tree(scene, b, wide, max_leaf)
+
+
+def test_host_tree_generated_scene():
+    scene = P.SceneData.generate(A.PHX_SCENE_CAUSTIC, 1, 64, 64, detail=16)
+    check_tree(scene, R.traversal_bvh(scene, 4, True, -1), True, 4)
+
+
+def test_traversal_build_rejects_bad_input():
+    scene = random_soup(10)
+    with pytest.raises(A.PhxError):
+        R.traversal_bvh(scene, 0, True, -1)
+    with pytest.raises(A.PhxError):
+        R.traversal_bvh(scene, 17, True, -1)
+
+
+# ---- GPU: the device build --------------------------------------------------------------------
+
+def gpu_cases():
+    return {
+        "one": lambda: random_soup(1, 3),
+        "two": lambda: random_soup(2, 4),
+        "soup_5k": lambda: random_soup(5000, 5),
+        "soup_40k_thin": lambda: random_soup(40000, 6, scale=50.0, size=0.05),
+        # > 2048 coincident centroids: the chunked (large-task) object-median path
+        "coincident_big": lambda: coincident_soup(5000, 3000),
+        "coincident_small": lambda: coincident_soup(70, 40),
+        "grid": lambda: grid_soup(128),
+        "cornell": lambda: P.SceneData.generate(A.PHX_SCENE_CORNELL, 1, 64, 64),
+        "caustic": lambda: P.SceneData.generate(A.PHX_SCENE_CAUSTIC, 1, 1024, 1024),
+        "atrium": lambda: P.SceneData.generate(A.PHX_SCENE_ATRIUM, 1, 1920, 1080),
+    }
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(gpu_cases()))
+def test_device_tree_equals_host(name):
+    scene = gpu_cases()[name]()
+    for wide, max_leaf in ((True, 4), (False, 4), (True, 1), (False, 16)):
+        h = R.traversal_bvh(scene, max_leaf, wide, -1)
+        d = R.traversal_bvh(scene, max_leaf, wide, 0)
+        tag = f"{name} wide={wide} leaf={max_leaf}"
+        assert (d.root, d.depth, d.wdepth) == (h.root, h.depth, h.wdepth), tag
+        assert d.nodes.shape == h.nodes.shape, tag
+        assert np.array_equal(d.nodes.view(np.uint32), h.nodes.view(np.uint32)), tag
+        assert np.array_equal(d.trirec.view(np.uint32), h.trirec.view(np.uint32)), tag
+        assert np.array_equal(d.leaf_tri, h.leaf_tri), tag
+    if name in ("caustic", "atrium"):
+        print(f"{name}: {scene.n_triangles} triangles, host {h.build_ms:.1f} ms, device {d.build_ms:.1f} ms")
+
+
+RENDER = {
+    # name: (kind, detail, width, height, photons, bounces, grid)
+    "cornell": (A.PHX_SCENE_CORNELL, 0, 64, 64, 1 << 14, 8, 50),
+    "caustic": (A.PHX_SCENE_CAUSTIC, 0, 96, 80, 1 << 15, 12, 50),
+    "atrium": (A.PHX_SCENE_ATRIUM, 16, 96, 54, 1 << 14, 16, 64),
+}
+
+
+def render(name, flags, rounds=3):
+    kind, detail, w, h, ph, mb, g = RENDER[name]
+    scene = P.SceneData.generate(kind, seed=1, width=w, height=h, detail=detail)
+    args = P.ArgsList(width=w, height=h, photons_per_round=ph, max_photon_bounces=mb, grid_res=g, seed=3,
+                      direct_samples=4, flags=flags)
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        r.iterate(rounds)
+        info = r.info()
+        return r.read("RADIANCE"), r.read("FLUX"), info
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(RENDER))
+@pytest.mark.parametrize("extra", [0, A.PHX_F_BINARY_BVH])
+def test_device_tree_renders_identically(name, extra):
+    rad_h, flux_h, ih = render(name, extra)
+    rad_d, flux_d, idv = render(name, extra | A.PHX_F_DEVICE_BVH)
+    assert (idv.trav_depth, idv.trav_inner_nodes) == (ih.trav_depth, ih.trav_inner_nodes)
+    assert idv.stack_overflows == ih.stack_overflows == 0
+    assert np.array_equal(rad_d.view(np.uint32), rad_h.view(np.uint32))
+    assert np.array_equal(flux_d.view(np.uint32), flux_h.view(np.uint32))
+    assert idv.bvh_build_ms > 0.0 and idv.setup_ms >= idv.bvh_build_ms
+
+
+@pytest.mark.gpu
+def test_device_tree_in_a_batch():
+    specs = [("cornell", 0), ("caustic", 0), ("atrium", 0)]
+    out = {}
+    for flags in (0, A.PHX_F_DEVICE_BVH):
+        scenes, args = [], []
+        for name, _ in specs:
+            kind, detail, w, h, ph, mb, g = RENDER[name]
+            scenes.append(P.SceneData.generate(kind, seed=2, width=w, height=h, detail=detail))
+            args.append(P.ArgsList(width=w, height=h, photons_per_round=ph, max_photon_bounces=mb, grid_res=g,
+                                   seed=5, direct_samples=4, flags=flags))
+        b = P.Batch(scenes, args)
+        b.iterate(2)
+        out[flags] = [b.read(i, "RADIANCE") for i in range(len(specs))]
+        b.close()
+    for a, d in zip(out[0], out[A.PHX_F_DEVICE_BVH]):
+        assert np.array_equal(a.view(np.uint32), d.view(np.uint32))
