@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <thread>
 
 namespace phx {
 
@@ -57,32 +58,28 @@ bool triangle_box(const phx_triangle &t, Box &b) {
     return true;
 }
 
-struct BuildNode {
-    Box box;
-    int32_t tri;
-    uint32_t left, right;
-};
-
+// build_tmp + flatten (bvh.cpp:18-72) in one pass: one triangle per leaf, median split of the
+// longest axis of the node box on the triangle boxes' minimum corner, written straight into the
+// flattened pre-order array.  A subtree over m triangles takes 2m-1 slots, so a node at slot p has
+// its left child at p+1 and its right child at p + 2*(mid-start): disjoint subtrees are written by
+// independent threads.  Each range is sorted exactly as the sequential build sorts it (same
+// comparator, same input order), so the nodes do not depend on the threading.
 struct Builder {
     const std::vector<Box> &boxes;
     std::vector<uint32_t> order;
-    std::vector<BuildNode> tmp;
+    phx_bvh_node *out;
 
-    explicit Builder(const std::vector<Box> &b) : boxes(b), order(b.size()) {
+    Builder(const std::vector<Box> &b, phx_bvh_node *o) : boxes(b), order(b.size()), out(o) {
         std::iota(order.begin(), order.end(), 0u);
-        tmp.reserve(2 * b.size());
     }
 
-    // build_tmp (bvh.cpp:18-53): one triangle per leaf, median split of the longest axis of the
-    // node box on the triangle boxes' minimum corner.
-    uint32_t build(uint32_t start, uint32_t end) {
-        uint32_t id = (uint32_t)tmp.size();
-        tmp.push_back({});
+    void build(uint32_t start, uint32_t end, uint32_t pos, int spawn_depth) {
+        phx_bvh_node &nd = out[pos];
         if (end == start + 1) {
-            tmp[id].tri = (int32_t)order[start];
-            tmp[id].box = boxes[order[start]];
-            tmp[id].left = tmp[id].right = 0;
-            return id;
+            const Box &bx = boxes[order[start]];
+            nd.min = {bx.lo[0], bx.lo[1], bx.lo[2], u2f(order[start])};
+            nd.max = {bx.hi[0], bx.hi[1], bx.hi[2], u2f(0u)};
+            return;
         }
         Box nb = boxes[order[start]];
         for (uint32_t i = start + 1; i < end; i++) {
@@ -92,8 +89,6 @@ struct Builder {
                 nb.hi[a] = std::max(nb.hi[a], o.hi[a]);
             }
         }
-        tmp[id].box = nb;
-        tmp[id].tri = -1;
         // get_longest_axis (bounding_box.h:63-78)
         float xs = nb.hi[0] - nb.lo[0], ys = nb.hi[1] - nb.lo[1], zs = nb.hi[2] - nb.lo[2];
         int axis = 2;
@@ -106,26 +101,17 @@ struct Builder {
         const std::vector<Box> &bx = boxes;
         std::sort(order.begin() + start, order.begin() + end,
                   [&bx, axis](uint32_t i, uint32_t j) { return bx[i].lo[axis] < bx[j].lo[axis]; });
-        uint32_t mid = start + (end - start) / 2;
-        uint32_t l = build(start, mid);
-        uint32_t r = build(mid, end);
-        tmp[id].left = l;
-        tmp[id].right = r;
-        return id;
-    }
-
-    // flatten (bvh.cpp:57-72): pre-order, left child follows its parent, right child index kept
-    // in max.w, triangle index (or -1) in min.w.
-    void flatten(uint32_t ti, std::vector<phx_bvh_node> &out) const {
-        uint32_t id = (uint32_t)out.size();
-        out.push_back({});
-        const BuildNode &n = tmp[ti];
-        out[id].min = {n.box.lo[0], n.box.lo[1], n.box.lo[2], u2f((uint32_t)n.tri)};
-        out[id].max = {n.box.hi[0], n.box.hi[1], n.box.hi[2], u2f(n.right)};
-        if (n.tri == -1) {
-            flatten(n.left, out);
-            out[id].max.w = u2f((uint32_t)out.size());
-            flatten(n.right, out);
+        const uint32_t mid = start + (end - start) / 2;
+        const uint32_t right = pos + 2 * (mid - start);
+        nd.min = {nb.lo[0], nb.lo[1], nb.lo[2], u2f(0xFFFFFFFFu)};
+        nd.max = {nb.hi[0], nb.hi[1], nb.hi[2], u2f(right)};
+        if (spawn_depth > 0 && end - start >= 4096) {
+            std::thread t([&] { build(start, mid, pos + 1, spawn_depth - 1); });
+            build(mid, end, right, spawn_depth - 1);
+            t.join();
+        } else {
+            build(start, mid, pos + 1, 0);
+            build(mid, end, right, 0);
         }
     }
 };
@@ -156,11 +142,13 @@ bool bvh_build(const phx_triangle *tris, uint32_t n, std::vector<phx_bvh_node> &
     for (uint32_t i = 0; i < n; i++)
         if (!triangle_box(tris[i], boxes[i]))
             return false;
-    Builder b(boxes);
-    b.build(0, n);
-    nodes.clear();
-    nodes.reserve(2 * (size_t)n - 1);
-    b.flatten(0, nodes);
+    nodes.assign(2 * (size_t)n - 1, phx_bvh_node{});
+    Builder b(boxes, nodes.data());
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    int spawn = 0;
+    while (spawn < 4 && (2u << spawn) <= hw)
+        spawn++;
+    b.build(0, n, 0, spawn);
     if (depth)
         *depth = depth_of(nodes, 0);
     return true;

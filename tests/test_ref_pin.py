@@ -133,13 +133,13 @@ def test_luminance_prefix_sums_are_the_reference_sums():
 
 
 @need_ref
-@pytest.mark.parametrize("seed", [1, 2, 3])
+@pytest.mark.parametrize("seed", [1, 2, 3, 4])
 def test_bvh_over_triangle_soups_is_the_reference_tree(seed):
     """Random triangles on a coarse lattice (many tied box minima, which the reference's
-    unstable std::sort orders) — the oracle's tree and the library's builder's interchange
-    format must equal the reference's bit for bit."""
+    unstable std::sort orders) — the oracle's tree and the library's builder (whose subtrees of
+    4096 triangles or more are built by parallel threads) must equal the reference's bit for bit."""
     rng = np.random.default_rng(seed)
-    n = [7, 300, 2500][seed - 1]
+    n = [7, 300, 2500, 40000][seed - 1]
     tris = (A.Triangle * n)()
     for t in tris:
         base = rng.integers(0, 6, 3) * 0.25
@@ -149,6 +149,10 @@ def test_bvh_over_triangle_soups_is_the_reference_tree(seed):
     want = R.bvh_build(C.addressof(tris), n)
     got, _ = O.bvh_build(C.addressof(tris), n)
     assert same_bits(got, want)
+    lib = (A.BvhNode * (2 * n - 1))()
+    depth = C.c_uint32()
+    A.check(A.load().phx_bvh_build(tris, n, lib, C.byref(depth)))
+    assert same_bits(np.frombuffer(bytes(lib), np.float32).reshape(2 * n - 1, 8), want)
 
 
 @need_ref
