@@ -49,9 +49,16 @@ CONFIGS = {
 }
 METRIC = "Mphotons/s"
 # dram__bytes_read.sum + dram__bytes_write.sum of a reference stage's kernels per round, from a
-# one-launch-per-kernel ncu capture of the workload at 1/2 resolution and 1/4 photons, scaled to the
-# full workload by pixels (trace_rays) or photon paths (emit_photons); None where not captured
-NCU_TRAFFIC: dict = {}
+# one-launch-per-kernel ncu capture of the caustic workload at 1/2 resolution and 1/4 photons
+# (512x512 pixels, 2^18 photon paths, 425,890 stored photons), scaled by 4 to the full workload
+# (pixels for trace_rays, photon paths or stored photons for the others; the 125,001-cell scan does
+# not scale).  trace_rays = k_trace_persistent 228.3 MB + k_shadow 158.6 + k_nee_resolve 77.7 +
+# k_spec_resolve 13.6; emit_photons = k_emit_persistent 130.1 + k_scan 1.1 + k_compact 28.6;
+# scatter_photons = the two radix passes 10.6 + k_sorted_records 11.9.  The integer stages' arrays
+# stay in the 126 MB L2 between kernels, so their DRAM bytes fall below the compulsory bytes.
+# gather_flux was captured only in its optional warp-cooperative form: left out.
+NCU_TRAFFIC: dict = {"caustic": {"trace_rays": 1912.9e6, "emit_photons": 639.0e6, "hash_photons": 28.3e6,
+                                 "scan": 0.51e6, "scatter_photons": 89.9e6}}
 
 
 def load_peaks() -> tuple[float, str]:
@@ -285,7 +292,8 @@ def run_ours(a, cfg: dict) -> dict | None:
         t = sum(stages[x] for x in parts)
         per_stage[k] = {"kernels": parts, "ms": round(t, 4), "algo_bytes": algo[k],
                         "gbs": round(algo[k] / (t * 1e-3) / 1e9, 1) if t > 0 else None,
-                        "frac": round(algo[k] / (t * 1e-3) / 1e9 / peak, 5) if t > 0 else None}
+                        "frac": round(algo[k] / (t * 1e-3) / 1e9 / peak, 5) if t > 0 else None,
+                        "traffic": NCU_TRAFFIC.get(a.config, {}).get(k) if a.scale == 1 else None}
     dom = max(per_stage, key=lambda k: per_stage[k]["ms"])
     achieved = algo[dom] / (per_stage[dom]["ms"] * 1e-3) / 1e9
     traffic = NCU_TRAFFIC.get(a.config, {}).get(dom) if a.scale == 1 else None
