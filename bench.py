@@ -609,6 +609,35 @@ def run_inverse(a) -> dict:
             "result": res, "clocks": clk.summary()}
 
 
+def scene_setup_times() -> dict:
+    """Scene setup of the caustic (149,862 triangles) and atrium (262,898) scenes: the traversal
+    tree built on the host and on the GPU (triangles resident on the device), and the whole
+    set_scene with either, as phx_info reports it (trees, uploads)."""
+    import numpy as np
+
+    import phosphor_b200 as P
+    from phosphor_b200 import _capi as A
+    res = {}
+    for name, kind, w, h in (("caustic", A.PHX_SCENE_CAUSTIC, 1024, 1024), ("atrium", A.PHX_SCENE_ATRIUM, 1920, 1080)):
+        scene = P.SceneData.generate(kind, seed=1, width=w, height=h)
+        host = P.traversal_bvh(scene, 4, True, -1)
+        P.traversal_bvh(scene, 4, True, 0)  # warm-up (module load, allocations)
+        dev = P.traversal_bvh(scene, 4, True, 0)
+        same = bool(np.array_equal(host.nodes.view(np.uint32), dev.nodes.view(np.uint32)) and
+                    np.array_equal(host.trirec.view(np.uint32), dev.trirec.view(np.uint32)))
+        row = {"triangles": scene.n_triangles, "traversal_tree_host_ms": round(host.build_ms, 2),
+               "traversal_tree_gpu_ms": round(dev.build_ms, 2), "identical": same}
+        for tag, flags in (("host", 0), ("gpu", A.PHX_F_DEVICE_BVH)):
+            args = P.ArgsList(width=w, height=h, photons_per_round=1 << 16, flags=flags)
+            with P.Renderer(args) as r:
+                r.set_scene(scene)
+                info = r.info()
+            row[f"set_scene_{tag}_ms"] = round(info.setup_ms, 1)
+            row[f"trees_{tag}_ms"] = round(info.bvh_build_ms, 1)
+        res[name] = row
+    return res
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -619,6 +648,7 @@ def main() -> int:
     ap.add_argument("--no-rmse", action="store_true", help="skip the time-to-RMSE study (1 GPU only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-inverse", action="store_true", help="skip the inverse-rendering block (1 GPU only)")
+    ap.add_argument("--no-setup", action="store_true", help="skip the scene-setup (tree build) timings")
     ap.add_argument("--simple", action="store_true", help="one-thread-per-item kernels instead of lane refill")
     ap.add_argument("--persistent", action="store_true", help="lane-refill state-machine kernels")
     ap.add_argument("--binary-bvh", action="store_true", help="traverse child pairs instead of 4-wide nodes")
@@ -669,6 +699,8 @@ def main() -> int:
     if out is not None:
         if not a.no_rmse and out["n_gpus"] == 1 and a.scale == 1:
             out["time_to_rmse"] = time_to_rmse_small(a)
+        if not a.no_setup and out["n_gpus"] == 1 and a.scale == 1:
+            out["scene_setup"] = scene_setup_times()
         if not a.no_inverse and out["n_gpus"] == 1 and a.scale == 1:
             # inverse rendering through the adjoint (atrium 512x512, 200 Adam steps)
             inv = run_inverse(a)

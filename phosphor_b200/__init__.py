@@ -5,7 +5,8 @@ the reference renderer's host API (ArgsList / Renderer / SceneData) on top of th
 """
 from . import _capi as capi
 from ._capi import PhxError, load
-from .renderer import ArgsList, Batch, Renderer, SceneData, bvh_build, camera_make, write_png
+from .renderer import (ArgsList, Batch, Renderer, SceneData, TraversalBvh, bvh_build, camera_make, traversal_bvh,
+                       write_png)
 
-__all__ = ["capi", "load", "PhxError", "ArgsList", "Renderer", "Batch", "SceneData", "bvh_build", "camera_make",
-           "write_png"]
+__all__ = ["capi", "load", "PhxError", "ArgsList", "Renderer", "Batch", "SceneData", "TraversalBvh", "bvh_build",
+           "camera_make", "traversal_bvh", "write_png"]
