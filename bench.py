@@ -233,6 +233,10 @@ def run_ours(a, cfg: dict) -> dict | None:
     args = make_args(cfg)
     if a.binary_bvh:
         args.flags = args.flags | 4  # PHX_F_BINARY_BVH
+    if a.quant_bvh:
+        args.flags = args.flags | 16  # PHX_F_QUANT_BVH
+    if a.device_bvh:
+        args.flags = args.flags | 8  # PHX_F_DEVICE_BVH
     if a.leaf_size:
         args.bvh_leaf_size = a.leaf_size
     scene = P.SceneData.generate(cfg["kind"], seed=1, width=args.width, height=args.height, detail=cfg["detail"])
@@ -453,10 +457,17 @@ def time_to_rmse_batch16(a) -> dict:
     if fx.exists():
         z = np.load(fx)
         small = [R.scaled(s, int(z["scale"])) for s in specs]
+        fp64 = [z[f"scene{i}"].astype(np.float64) / 65535.0 for i in range(len(small))]
         imgs = R.batch_images(small, TTR_REF_ROUNDS, seed_offset=TTR_CAL_SEED_OFFSET, pipeline=TTR_PIPELINE)
-        cal_rmse = [R.rmse(img, z[f"scene{i}"].astype(np.float64) / 65535.0) for i, img in enumerate(imgs)]
+        cal_rmse = [R.rmse(img, ref) for img, ref in zip(imgs, fp64)]
+        # the same photon and camera paths (the FP64 images' seeds and round count): what remains is
+        # the arithmetic, fp32 on the GPU against double precision
+        same = R.batch_images(small, int(z["rounds"]), seed_offset=R.RMSE_REF_SEED_OFFSET, pipeline=TTR_PIPELINE)
+        same_rmse = [R.rmse(img, ref) for img, ref in zip(same, fp64)]
         cal = {"scale": int(z["scale"]), "fp64_rounds": int(z["rounds"]), "fp32_rounds": TTR_REF_ROUNDS,
-               "rmse_fp32_ref_vs_fp64": [round(x, 5) for x in cal_rmse], "max": round(max(cal_rmse), 5)}
+               "rmse_fp32_ref_vs_fp64": [round(x, 5) for x in cal_rmse], "max": round(max(cal_rmse), 5),
+               "rmse_fp32_vs_fp64_same_paths": [round(x, 6) for x in same_rmse],
+               "max_same_paths": round(max(same_rmse), 6)}
     r_star, curve = R.rounds_to_target(specs, refs, TTR_TARGET, TTR_MAX_ROUNDS, TTR_CHECK)
     capped = [i for i, r in enumerate(r_star) if r is None]
     r_eff = [TTR_MAX_ROUNDS if r is None else r for r in r_star]
@@ -464,6 +475,12 @@ def time_to_rmse_batch16(a) -> dict:
     t_plain = sum(dt for dt, _ in plain)
     plain_rmse = [R.rmse(img, ref) for (_, img), ref in zip(plain, refs)]
     t_batch = R.time_batched_schedule(specs, r_eff, pipeline=TTR_PIPELINE)
+    # the scenes that reach the target, alone: the stalled ones (alpha near 0.6: the radius
+    # re-initialisation of gather_flux.cl:50-56) never do, in any form
+    conv = [i for i, r in enumerate(r_star) if r is not None]
+    t_plain_conv = sum(plain[i][0] for i in conv)
+    t_batch_conv = R.time_batched_schedule([specs[i] for i in conv], [r_star[i] for i in conv],
+                                           pipeline=TTR_PIPELINE) if conv else None
     # the reference's kernel shapes (one thread per item, its median-split tree, NEE inline), per
     # round on a 20-round sample of each scene: a secondary, extrapolated comparison
     t_ref_shape = sum(r * R.time_plain(s, 20, reference_shaped=True) for s, r in zip(specs, r_eff))
@@ -478,6 +495,10 @@ def time_to_rmse_batch16(a) -> dict:
             "plain_final_rmse": [round(x, 5) for x in plain_rmse],
             "plain_s": round(t_plain, 3), "plain_s_per_scene": [round(dt, 3) for dt, _ in plain],
             "graph_batched_s": round(t_batch, 3), "speedup": round(t_plain / t_batch, 3),
+            "alpha": [round(sp.alpha, 4) for sp in specs], "converging_scenes": conv,
+            "converging_plain_s": round(t_plain_conv, 3),
+            "converging_graph_batched_s": round(t_batch_conv, 3) if t_batch_conv else None,
+            "converging_speedup": round(t_plain_conv / t_batch_conv, 3) if t_batch_conv else None,
             "plain_reference_shaped_s_extrapolated": round(t_ref_shape, 2),
             "speedup_vs_reference_shaped": round(t_ref_shape / t_batch, 2)}
 
@@ -652,6 +673,8 @@ def main() -> int:
     ap.add_argument("--simple", action="store_true", help="one-thread-per-item kernels instead of lane refill")
     ap.add_argument("--persistent", action="store_true", help="lane-refill state-machine kernels")
     ap.add_argument("--binary-bvh", action="store_true", help="traverse child pairs instead of 4-wide nodes")
+    ap.add_argument("--quant-bvh", action="store_true", help="4-wide nodes with 8-bit child boxes")
+    ap.add_argument("--device-bvh", action="store_true", help="build the traversal tree on the GPU")
     ap.add_argument("--leaf-size", type=int, default=0, help="triangles per leaf of the traversal tree (0: library default)")
     ap.add_argument("--autotune", action="store_true", help="run the library autotuner before timing")
     ap.add_argument("--shard", action="store_true",

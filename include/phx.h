@@ -163,6 +163,7 @@ typedef struct phx_params {
 #define PHX_F_SIMPLE_TRAVERSAL 1u /* one-thread-per-ray kernels instead of the persistent ones */
 #define PHX_F_REFERENCE_BVH 2u    /* traverse the reference's median-split tree instead of the SAH tree */
 #define PHX_F_BINARY_BVH 4u       /* traverse the SAH tree as child pairs instead of 4-wide nodes */
+#define PHX_F_QUANT_BVH 16u       /* 4-wide nodes with 8-bit child boxes (64 instead of 112 bytes) */
 #define PHX_F_DEVICE_BVH 8u       /* build the SAH traversal tree on the GPU (the same tree, bit for
                                      bit; the reference tree for tie-break ranks is built on the host
                                      meanwhile) */
@@ -275,8 +276,9 @@ PHX_API int phx_image(void *ctx, float exposure, int tonemap, uint64_t total_pho
 PHX_API int phx_bvh_build(const phx_triangle *tris, uint32_t n, phx_bvh_node *out_nodes, uint32_t *depth);
 /* The traversal tree the kernels walk (no reference counterpart: the reference traverses the tree of
  * bvh.cpp): a binned-SAH tree over the reference's expanded triangle boxes with leaves of up to
- * max_leaf (1..16) triangles, as child pairs (16 floats per inner node) or collapsed to 4-wide
- * nodes (28 floats), each triangle record (12 floats, leaf order) carrying its leaf rank in the
+ * max_leaf (1..16) triangles, as child pairs (wide = 0: 16 floats per inner node), collapsed to
+ * 4-wide nodes (wide = 1: 28 floats) or 4-wide nodes with 8-bit child boxes (wide = 2: 16 words),
+ * each triangle record (12 floats, leaf order) carrying its leaf rank in the
  * reference tree.  device < 0 builds on the host; device >= 0 builds on that GPU (PHX_F_DEVICE_BVH)
  * and returns the same arrays bit for bit.  nodes needs room for 16 (or 28) floats per triangle,
  * trirec 12 floats and leaf_tri one entry per triangle.  build_ms: wall time of the traversal tree

@@ -204,13 +204,15 @@ PHX_API int phx_bvh_build(const phx_triangle *tris, uint32_t n, phx_bvh_node *ou
 PHX_API int phx_traversal_bvh_build(const phx_triangle *tris, uint32_t n, uint32_t max_leaf, int wide, int device,
                                     phx_bvh_packed *out) {
     return guard([&]() -> int {
-        if (!tris || !out || !out->nodes || !out->trirec || !out->leaf_tri || n == 0 || max_leaf < 1 || max_leaf > 16)
+        if (!tris || !out || !out->nodes || !out->trirec || !out->leaf_tri || n == 0 || max_leaf < 1 ||
+            max_leaf > 16 || wide < 0 || wide > 2)
             return fail(PHX_E_INVALID, "bad arguments");
+        const bool quant = wide == 2;
         std::vector<phx_bvh_node> ref;
         if (!bvh_build(tris, n, ref, nullptr))
             return fail(PHX_E_INVALID, "degenerate or infinite triangle bounding box");
         const std::vector<uint32_t> ranks = reference_leaf_ranks(ref, n);
-        const uint32_t per = wide ? 28u : 16u;
+        const uint32_t per = quant ? 16u : wide ? 28u : 16u;
         if (device < 0) {
             const auto t0 = std::chrono::steady_clock::now();
             PackedBvh pk;
@@ -218,12 +220,18 @@ PHX_API int phx_traversal_bvh_build(const phx_triangle *tris, uint32_t n, uint32
                 return fail(PHX_E_INVALID, "SAH build failed");
             if (wide)
                 bvh_widen(pk);
+            std::vector<uint32_t> qn;
+            if (quant)
+                qn = bvh_quantize(pk);
             out->build_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
             const std::vector<float> &nodes = wide ? pk.wnodes : pk.cnodes;
-            std::memcpy(out->nodes, nodes.data(), nodes.size() * 4);
+            if (quant)
+                std::memcpy(out->nodes, qn.data(), qn.size() * 4);
+            else
+                std::memcpy(out->nodes, nodes.data(), nodes.size() * 4);
             std::memcpy(out->trirec, pk.trirec.data(), pk.trirec.size() * 4);
             std::memcpy(out->leaf_tri, pk.leaf_tri.data(), pk.leaf_tri.size() * 4);
-            out->n_nodes = (uint32_t)(nodes.size() / per);
+            out->n_nodes = (uint32_t)(nodes.size() / (wide ? 28u : 16u));
             out->root = wide ? pk.wroot : pk.root;
             out->depth = pk.depth;
             out->wdepth = wide ? pk.wdepth : 0u;
@@ -256,7 +264,8 @@ PHX_API int phx_traversal_bvh_build(const phx_triangle *tris, uint32_t n, uint32
         auto *d_nrm = static_cast<float4 *>(dalloc(48 * (size_t)n));
         auto *d_tan = static_cast<float4 *>(dalloc(48 * (size_t)n));
         auto *d_uv = static_cast<float4 *>(dalloc(32 * (size_t)n));
-        if (!d_tris || !d_rank || !d_rec || !d_nrm || !d_tan || !d_uv)
+        auto *d_q = static_cast<uint32_t *>(dalloc(quant ? 64 * (size_t)n : 16));
+        if (!d_tris || !d_rank || !d_rec || !d_nrm || !d_tan || !d_uv || !d_q)
             return fail(PHX_E_OOM, "device allocation failed");
         CK(cudaMemcpy(d_tris, tris, sizeof(phx_triangle) * (size_t)n, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(d_rank, ranks.data(), 4 * (size_t)n, cudaMemcpyHostToDevice));
@@ -267,6 +276,8 @@ PHX_API int phx_traversal_bvh_build(const phx_triangle *tris, uint32_t n, uint32
             return fail(rc == 2 ? PHX_E_OOM : rc == 1 ? PHX_E_INVALID : PHX_E_CUDA, msg);
         if (bvh_device_finish(d_tris, d_rank, n, c.db, d_rec, d_nrm, d_tan, d_uv, st))
             return fail(PHX_E_CUDA, "device BVH triangle records: launch failed");
+        if (quant && c.db.n_wide)
+            CK(bvh_device_quantize(c.db.wnodes, c.db.n_wide, d_q, st));
         CK(cudaStreamSynchronize(st));
         out->build_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
         out->n_nodes = wide ? c.db.n_wide : c.db.n_inner;
@@ -274,8 +285,8 @@ PHX_API int phx_traversal_bvh_build(const phx_triangle *tris, uint32_t n, uint32
         out->depth = c.db.depth;
         out->wdepth = wide ? c.db.wdepth : 0u;
         if (out->n_nodes)
-            CK(cudaMemcpy(out->nodes, wide ? c.db.wnodes : c.db.cnodes, (size_t)out->n_nodes * per * 4,
-                          cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(out->nodes, quant ? (const void *)d_q : wide ? (const void *)c.db.wnodes : c.db.cnodes,
+                          (size_t)out->n_nodes * per * 4, cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(out->trirec, d_rec, 48 * (size_t)n, cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(out->leaf_tri, c.db.leaf_tri, 4 * (size_t)n, cudaMemcpyDeviceToHost));
         return PHX_OK;

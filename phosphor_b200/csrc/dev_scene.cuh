@@ -64,7 +64,8 @@ struct __align__(16) SceneDesc {
     u32 pixel_base;       // first pixel of this scene
     u32 emit_base;        // first photon path of this scene
     u32 cell_base;        // first cell of this scene
-    u32 wide;             // 1: cnodes holds 4-wide nodes (7 float4 each), 0: child pairs (4 float4)
+    u32 wide;             // 2: 4-wide nodes with 8-bit child boxes (4 uint4 each), 1: 4-wide nodes (7
+                          // float4), 0: child pairs (4 float4)
     u64 slot_base;        // first photon slot of this scene (slot j of path t at slot_base + j*n_emit + t)
     u32 flags;
     u32 any_transmissive; // 0 -> shadow rays can stop at the first hit
@@ -180,6 +181,21 @@ PHX_DI float box1(float nx, float fx, float ny, float fy, float nz, float fz, fl
     return tn <= tf ? tn : __int_as_float(0x7f800000);
 }
 
+// Byte k of w as a float: the byte under the exponent of 2^23, minus 2^23 (exact).
+PHX_DI float qbyte(u32 w, int k) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440 + k)) - 8388608.0f; }
+
+// Slab test of child k of an 8-bit node: per axis the entry and exit byte words (picked by the
+// direction's sign), the distance of one quantisation step (s) and of the node origin (b); the plane
+// of byte q lies at distance q * s + b.  Returns the entry distance, or +inf on a miss.
+PHX_DI float qbox(u32 nxw, u32 fxw, u32 nyw, u32 fyw, u32 nzw, u32 fzw, int k, float sx, float sy, float sz, float bx,
+                  float by, float bz, float t_min, float t_max) {
+    const float tn = fmaxf(fmaxf(__fmaf_rn(qbyte(nxw, k), sx, bx), __fmaf_rn(qbyte(nyw, k), sy, by)),
+                           fmaxf(__fmaf_rn(qbyte(nzw, k), sz, bz), t_min));
+    const float tf = fminf(fminf(__fmaf_rn(qbyte(fxw, k), sx, bx), __fmaf_rn(qbyte(fyw, k), sy, by)),
+                           fminf(__fmaf_rn(qbyte(fzw, k), sz, bz), t_max));
+    return tn <= tf ? tn : __int_as_float(0x7f800000);
+}
+
 // The slab tests' inverse direction component 1/dc, except that the +-inf of a zero component
 // becomes +-1e30 while the origin's coordinate oc is below 1e4 in magnitude.  A ray with dc = 0
 // keeps the coordinate oc.  With +-inf, every plane on the same side of zero as oc gave
@@ -291,25 +307,47 @@ PHX_DI bool intersect_t(const SceneDesc &sc, float4 o, float4 d, float t_min, fl
         if (done)
             continue;
         if (node >= 0 && sc.wide) { // 4-wide node: descend into the nearest hit child, stack the rest
-            const float4 *wn = sc.cnodes + 7 * (size_t)node;
-            const float4 mnx = __ldg(wn + px), mxx = __ldg(wn + (1 - px)), mny = __ldg(wn + py);
-            const float4 mxy = __ldg(wn + (5 - py)), mnz = __ldg(wn + pz), mxz = __ldg(wn + (9 - pz));
-            const int4 ch = __ldg(reinterpret_cast<const int4 *>(wn + 6));
-            // (mnx.. now hold the entry planes, mxx.. the exit planes.)  An empty slot (reference POP)
-            // never counts as hit, whatever its box.
             const float NOHIT = __int_as_float(0x7f800000);
-            float t0 = ch.x == POP ? NOHIT
-                                   : box1(mnx.x, mxx.x, mny.x, mxy.x, mnz.x, mxz.x, ix, iy, iz, oix, oiy, oiz, t_min,
-                                          closest);
-            float t1 = ch.y == POP ? NOHIT
-                                   : box1(mnx.y, mxx.y, mny.y, mxy.y, mnz.y, mxz.y, ix, iy, iz, oix, oiy, oiz, t_min,
-                                          closest);
-            float t2 = ch.z == POP ? NOHIT
-                                   : box1(mnx.z, mxx.z, mny.z, mxy.z, mnz.z, mxz.z, ix, iy, iz, oix, oiy, oiz, t_min,
-                                          closest);
-            float t3 = ch.w == POP ? NOHIT
-                                   : box1(mnx.w, mxx.w, mny.w, mxy.w, mnz.w, mxz.w, ix, iy, iz, oix, oiy, oiz, t_min,
-                                          closest);
+            float t0, t1, t2, t3;
+            int4 ch;
+            if (sc.wide == 2) { // 8-bit child boxes (bvh_quant.hpp)
+                const uint4 *qn = reinterpret_cast<const uint4 *>(sc.cnodes) + 4 * (size_t)node;
+                const uint4 h = __ldg(qn), qx = __ldg(qn + 1), qz = __ldg(qn + 2);
+                ch = __ldg(reinterpret_cast<const int4 *>(qn + 3));
+                // per axis: distance of the origin plane and of one step; entry / exit bytes by sign
+                const float sx = __uint_as_float((h.w & 0xffu) << 23) * ix;
+                const float sy = __uint_as_float(((h.w >> 8) & 0xffu) << 23) * iy;
+                const float sz = __uint_as_float(((h.w >> 16) & 0xffu) << 23) * iz;
+                const float bx = __fmaf_rn(__uint_as_float(h.x), ix, -oix);
+                const float by = __fmaf_rn(__uint_as_float(h.y), iy, -oiy);
+                const float bz = __fmaf_rn(__uint_as_float(h.z), iz, -oiz);
+                const u32 nxw = px == 0 ? qx.x : qx.y, fxw = px == 0 ? qx.y : qx.x;
+                const u32 nyw = py == 2 ? qx.z : qx.w, fyw = py == 2 ? qx.w : qx.z;
+                const u32 nzw = pz == 4 ? qz.x : qz.y, fzw = pz == 4 ? qz.y : qz.x;
+                t0 = ch.x == POP ? NOHIT : qbox(nxw, fxw, nyw, fyw, nzw, fzw, 0, sx, sy, sz, bx, by, bz, t_min, closest);
+                t1 = ch.y == POP ? NOHIT : qbox(nxw, fxw, nyw, fyw, nzw, fzw, 1, sx, sy, sz, bx, by, bz, t_min, closest);
+                t2 = ch.z == POP ? NOHIT : qbox(nxw, fxw, nyw, fyw, nzw, fzw, 2, sx, sy, sz, bx, by, bz, t_min, closest);
+                t3 = ch.w == POP ? NOHIT : qbox(nxw, fxw, nyw, fyw, nzw, fzw, 3, sx, sy, sz, bx, by, bz, t_min, closest);
+            } else {
+                const float4 *wn = sc.cnodes + 7 * (size_t)node;
+                const float4 mnx = __ldg(wn + px), mxx = __ldg(wn + (1 - px)), mny = __ldg(wn + py);
+                const float4 mxy = __ldg(wn + (5 - py)), mnz = __ldg(wn + pz), mxz = __ldg(wn + (9 - pz));
+                ch = __ldg(reinterpret_cast<const int4 *>(wn + 6));
+                // (mnx.. now hold the entry planes, mxx.. the exit planes.)  An empty slot (reference
+                // POP) never counts as hit, whatever its box.
+                t0 = ch.x == POP ? NOHIT
+                                 : box1(mnx.x, mxx.x, mny.x, mxy.x, mnz.x, mxz.x, ix, iy, iz, oix, oiy, oiz, t_min,
+                                        closest);
+                t1 = ch.y == POP ? NOHIT
+                                 : box1(mnx.y, mxx.y, mny.y, mxy.y, mnz.y, mxz.y, ix, iy, iz, oix, oiy, oiz, t_min,
+                                        closest);
+                t2 = ch.z == POP ? NOHIT
+                                 : box1(mnx.z, mxx.z, mny.z, mxy.z, mnz.z, mxz.z, ix, iy, iz, oix, oiy, oiz, t_min,
+                                        closest);
+                t3 = ch.w == POP ? NOHIT
+                                 : box1(mnx.w, mxx.w, mny.w, mxy.w, mnz.w, mxz.w, ix, iy, iz, oix, oiy, oiz, t_min,
+                                        closest);
+            }
             i32 r0 = ch.x, r1 = ch.y, r2 = ch.z, r3 = ch.w;
             if constexpr (!ORDERED) {
                 // slot order: descend into the first hit child, stack the other hit ones

@@ -188,8 +188,9 @@ static int device_traversal(SceneSlot &S, const phx_scene &s, const phx_params &
         return PHX_OK;
     }
     wide = want_wide && 3 * db.wdepth + 4 < (uint32_t)TRAV_STACK;
+    const bool quant = wide && (p.flags & PHX_F_QUANT_BVH);
     const float *nodes = wide ? db.wnodes : db.cnodes;
-    const uint32_t n_nodes = wide ? db.n_wide : db.n_inner, per = wide ? 28u : 16u;
+    const uint32_t n_nodes = wide ? db.n_wide : db.n_inner, per = quant ? 16u : wide ? 28u : 16u;
     S.trav_depth = wide ? db.wdepth : db.depth;
     S.trav_inner = n_nodes;
     root = wide ? db.wroot : db.root;
@@ -198,7 +199,9 @@ static int device_traversal(SceneSlot &S, const phx_scene &s, const phx_params &
         (r = S.bufs[3].alloc((size_t)n * 48)) || (r = S.bufs[4].alloc((size_t)n * 32)) ||
         (r = upload(rank, ranks.data(), 4 * (size_t)n)))
         return r;
-    if (n_nodes)
+    if (n_nodes && quant)
+        CK(bvh_device_quantize(db.wnodes, n_nodes, S.bufs[0].as<u32>(), st));
+    else if (n_nodes)
         CK(cudaMemcpyAsync(S.bufs[0].p, nodes, (size_t)n_nodes * per * 4, cudaMemcpyDeviceToDevice, st));
     if (bvh_device_finish(tris.as<phx_triangle>(), rank.as<u32>(), n, db, S.bufs[1].as<float4>(),
                           S.bufs[2].as<float4>(), S.bufs[3].as<float4>(), S.bufs[4].as<float4>(), st))
@@ -257,6 +260,7 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
     if ((p.flags & PHX_F_DEVICE_BVH) && !(p.flags & PHX_F_REFERENCE_BVH) &&
         (r = device_traversal(S, s, p, st, ref_built, trav_done, force_ref, trav_root, wide)))
         return r;
+    const bool quant_req = (p.flags & PHX_F_QUANT_BVH) != 0;
     if (!trav_done) {
         if (!ref_built && !bvh_build(s.triangles, s.n_triangles, S.nodes, &S.depth))
             return fail(PHX_E_INVALID, "degenerate or infinite triangle bounding box (bounding_box.h:17-28)");
@@ -292,8 +296,14 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
             float u8v[8] = {t.uv0.x, t.uv0.y, t.uv1.x, t.uv1.y, t.uv2.x, t.uv2.y, 0.0f, 0.0f};
             std::memcpy(&uv[(size_t)k * 8], u8v, 32);
         }
-        const std::vector<float> &inner = wide ? pk.wnodes : pk.cnodes;
-        if ((r = upload(S.bufs[0], inner.data(), std::max<size_t>(inner.size(), 4) * 4)) ||
+        std::vector<uint32_t> qn;
+        if (wide && quant_req)
+            qn = bvh_quantize(pk);
+        const void *inner = wide && quant_req ? (const void *)qn.data()
+                            : wide           ? (const void *)pk.wnodes.data()
+                                             : (const void *)pk.cnodes.data();
+        const size_t inner_words = wide && quant_req ? qn.size() : wide ? pk.wnodes.size() : pk.cnodes.size();
+        if ((r = upload(S.bufs[0], inner, std::max<size_t>(inner_words, 4) * 4)) ||
             (r = upload(S.bufs[1], pk.trirec.data(), pk.trirec.size() * 4)) ||
             (r = upload(S.bufs[2], nrm.data(), nrm.size() * 4)) ||
             (r = upload(S.bufs[3], tan.data(), tan.size() * 4)) || (r = upload(S.bufs[4], uv.data(), uv.size() * 4)))
@@ -367,7 +377,7 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
     d.lum_pref_sum = S.bufs[14].as<float>();
     d.envmap = S.bufs[15].as<float>();
     d.root = trav_root;
-    d.wide = wide ? 1u : 0u;
+    d.wide = wide ? (quant_req ? 2u : 1u) : 0u;
     d.n_tris = n;
     d.n_lights = s.n_lights;
     d.total_lum = s.n_lights ? lum[s.n_lights - 1] : 0.0f; // shading.cpp:26

@@ -1,5 +1,6 @@
 // host.cpp — BVH construction and packing, photon-grid box and scene sphere.
 #include "host.hpp"
+#include "bvh_quant.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -474,6 +475,14 @@ void bvh_widen(PackedBvh &pk) {
             if (ch[k].ref >= 0)
                 work.push_back({ch[k].ref, w, k, it.depth + 1});
     }
+}
+
+std::vector<uint32_t> bvh_quantize(const PackedBvh &pk) {
+    const size_t n = pk.wnodes.size() / 28;
+    std::vector<uint32_t> q(n * QNODE_WORDS);
+    for (size_t w = 0; w < n; w++)
+        quantize_wide_node(&pk.wnodes[w * 28], &q[w * QNODE_WORDS]);
+    return q;
 }
 
 // build_photon_hash_info (photon_hash.h:41-50)

@@ -41,6 +41,8 @@ bool bvh_build_sah(const phx_triangle *tris, uint32_t n, const std::vector<uint3
 // maxy[4], minz[4], maxz[4], refs[4]}; an empty slot has reference 0x7fffffff (which traversal
 // checks: its inverted box would not by itself make the slab test miss).
 void bvh_widen(PackedBvh &pk);
+// The 4-wide nodes with 8-bit child boxes (bvh_quant.hpp), 16 words per node.
+std::vector<uint32_t> bvh_quantize(const PackedBvh &pk);
 
 phx_photon_hash_data hash_info(const phx_bvh_node &root, uint32_t grid_res);
 void scene_sphere(const phx_bvh_node &root, phx_f4 *center, float *radius);

@@ -28,6 +28,7 @@
 #include <cstring>
 #include <vector>
 
+#include "bvh_quant.hpp"
 #include "kernels.hpp"
 
 namespace phx {
@@ -909,6 +910,12 @@ __global__ void k_tri_records(const phx_triangle *tris, const u32 *leaf_tri, con
     uv[2 * (size_t)r + 1] = make_float4(t.uv2.x, t.uv2.y, 0.0f, 0.0f);
 }
 
+__global__ void k_quantize(const float *wnodes, u32 n, u32 *out) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        quantize_wide_node(wnodes + (size_t)i * 28, out + (size_t)i * QNODE_WORDS);
+}
+
 __global__ void k_push_root(BuildArgs A, u32 n) { push_task(A, 0, n, NO_PARENT, 0); }
 
 u32 blocks_for(u64 n, u32 bs) { return (u32)std::max<u64>(1, (n + bs - 1) / bs); }
@@ -1154,6 +1161,11 @@ int bvh_device_build(const phx_triangle *tris, u32 n, u32 max_leaf, bool widen, 
         return 3;
     }
     return 0;
+}
+
+cudaError_t bvh_device_quantize(const float *wnodes, u32 n, u32 *out, cudaStream_t st) {
+    k_quantize<<<blocks_for(n, 128), 128, 0, st>>>(wnodes, n, out);
+    return cudaGetLastError();
 }
 
 int bvh_device_finish(const phx_triangle *tris, const u32 *rank, u32 n, DeviceBvh &b, float4 *trirec, float4 *nrm,

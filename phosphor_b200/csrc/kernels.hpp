@@ -126,6 +126,8 @@ struct DeviceBvh {
 };
 int bvh_device_build(const phx_triangle *tris, u32 n, u32 max_leaf, bool widen, cudaStream_t st, DeviceBvh &out,
                      std::string &err);
+// 4-wide nodes -> 8-bit child boxes (bvh_quant.hpp), one thread per node
+cudaError_t bvh_device_quantize(const float *wnodes, u32 n, u32 *out, cudaStream_t st);
 int bvh_device_finish(const phx_triangle *tris, const u32 *rank, u32 n, DeviceBvh &b, float4 *trirec, float4 *nrm,
                       float4 *tan, float4 *uv, cudaStream_t st);
 

@@ -174,12 +174,14 @@ class TraversalBvh:
     build_ms: float
 
 
-def traversal_bvh(scene: SceneData, max_leaf: int = 4, wide: bool = True, device: int = -1) -> TraversalBvh:
-    """The SAH traversal tree the kernels walk, built on the host (device < 0) or on a GPU."""
+def traversal_bvh(scene: SceneData, max_leaf: int = 4, wide: int = 1, device: int = -1) -> TraversalBvh:
+    """The SAH traversal tree the kernels walk, built on the host (device < 0) or on a GPU.
+    wide: 0 child pairs (16 floats per node), 1 4-wide nodes (28 floats), 2 4-wide nodes with 8-bit
+    child boxes (16 words)."""
     lib = A.load()
     n = scene.scene.n_triangles
-    per = 28 if wide else 16
-    nodes = np.zeros((max(n, 1), per), np.float32)
+    per = 28 if int(wide) == 1 else 16
+    nodes = np.zeros((max(n, 1), 28), np.float32)
     trirec = np.zeros((n, 12), np.float32)
     leaf = np.zeros(n, np.uint32)
     out = A.BvhPacked()
@@ -187,7 +189,8 @@ def traversal_bvh(scene: SceneData, max_leaf: int = 4, wide: bool = True, device
     out.trirec = trirec.ctypes.data_as(C.POINTER(C.c_float))
     out.leaf_tri = leaf.ctypes.data_as(C.POINTER(C.c_uint32))
     A.check(lib.phx_traversal_bvh_build(scene.scene.triangles, n, max_leaf, int(wide), device, C.byref(out)))
-    return TraversalBvh(nodes[:out.n_nodes].copy(), trirec, leaf, out.root, out.depth, out.wdepth, out.build_ms)
+    flat = nodes.reshape(-1)[:out.n_nodes * per].reshape(out.n_nodes, per).copy()
+    return TraversalBvh(flat, trirec, leaf, out.root, out.depth, out.wdepth, out.build_ms)
 
 
 def camera_make(position, look_at, up, hfov_deg, aspect, defocus_angle=0.0, focus_distance=1.0) -> A.CameraParams:

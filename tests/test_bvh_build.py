@@ -144,12 +144,52 @@ def test_host_tree_generated_scene():
     check_tree(scene, R.traversal_bvh(scene, 4, True, -1), True, 4)
 
 
+def decode_qnodes(q: np.ndarray):
+    """8-bit nodes -> (lo, hi) per child (float64, exact) and refs, for the containment check."""
+    w = q.view(np.uint32)
+    P = w[:, 0:3].view(np.float32).astype(np.float64)
+    e = np.stack([(w[:, 3] >> (8 * a)) & 0xFF for a in range(3)], 1).astype(np.int64) - 127
+    step = np.ldexp(1.0, e)
+    lo = np.zeros((len(w), 4, 3))
+    hi = np.zeros((len(w), 4, 3))
+    for a in range(3):
+        for k in range(4):
+            lo[:, k, a] = P[:, a] + ((w[:, 4 + 2 * a] >> (8 * k)) & 0xFF) * step[:, a]
+            hi[:, k, a] = P[:, a] + ((w[:, 5 + 2 * a] >> (8 * k)) & 0xFF) * step[:, a]
+    return lo, hi, w[:, 12:16].view(np.int32), step
+
+
+@pytest.mark.parametrize("scene_fn", [lambda: random_soup(4000, 9, scale=30.0, size=0.02),
+                                      lambda: coincident_soup(300, 500),
+                                      lambda: P.SceneData.generate(A.PHX_SCENE_ATRIUM, 1, 64, 64, detail=16)])
+def test_quantized_nodes_contain_the_exact_boxes(scene_fn):
+    """Every 8-bit child box contains its float box (rounded outward by less than one step), and
+    the quantised tree has the 4-wide tree's topology."""
+    scene = scene_fn()
+    w = R.traversal_bvh(scene, 4, 1, -1)
+    q = R.traversal_bvh(scene, 4, 2, -1)
+    assert (q.root, q.depth, q.wdepth) == (w.root, w.depth, w.wdepth)
+    assert np.array_equal(q.trirec.view(np.uint32), w.trirec.view(np.uint32))
+    lo_q, hi_q, refs, step = decode_qnodes(q.nodes)
+    refs_w = w.nodes[:, 24:28].view(np.int32)
+    assert np.array_equal(refs, refs_w)
+    valid = refs_w != EMPTY
+    for a in range(3):
+        lo_w = w.nodes[:, 8 * a:8 * a + 4].astype(np.float64)
+        hi_w = w.nodes[:, 8 * a + 4:8 * a + 8].astype(np.float64)
+        assert np.all(lo_q[:, :, a][valid] <= lo_w[valid])
+        assert np.all(hi_q[:, :, a][valid] >= hi_w[valid])
+        s = np.broadcast_to(step[:, a:a + 1], lo_w.shape)
+        assert np.all(lo_w[valid] - lo_q[:, :, a][valid] < s[valid])
+        assert np.all(hi_q[:, :, a][valid] - hi_w[valid] < s[valid])
+
+
 def test_traversal_build_rejects_bad_input():
     scene = random_soup(10)
     with pytest.raises(A.PhxError):
-        R.traversal_bvh(scene, 0, True, -1)
+        R.traversal_bvh(scene, 0, 1, -1)
     with pytest.raises(A.PhxError):
-        R.traversal_bvh(scene, 17, True, -1)
+        R.traversal_bvh(scene, 17, 1, -1)
 
 
 # ---- GPU: the device build --------------------------------------------------------------------
@@ -174,7 +214,7 @@ def gpu_cases():
 @pytest.mark.parametrize("name", list(gpu_cases()))
 def test_device_tree_equals_host(name):
     scene = gpu_cases()[name]()
-    for wide, max_leaf in ((True, 4), (False, 4), (True, 1), (False, 16)):
+    for wide, max_leaf in ((1, 4), (0, 4), (1, 1), (0, 16), (2, 4)):
         h = R.traversal_bvh(scene, max_leaf, wide, -1)
         d = R.traversal_bvh(scene, max_leaf, wide, 0)
         tag = f"{name} wide={wide} leaf={max_leaf}"
@@ -183,8 +223,8 @@ def test_device_tree_equals_host(name):
         assert np.array_equal(d.nodes.view(np.uint32), h.nodes.view(np.uint32)), tag
         assert np.array_equal(d.trirec.view(np.uint32), h.trirec.view(np.uint32)), tag
         assert np.array_equal(d.leaf_tri, h.leaf_tri), tag
-    if name in ("caustic", "atrium"):
-        print(f"{name}: {scene.n_triangles} triangles, host {h.build_ms:.1f} ms, device {d.build_ms:.1f} ms")
+        if name in ("caustic", "atrium"):
+            print(f"{tag}: {scene.n_triangles} triangles, host {h.build_ms:.1f} ms, device {d.build_ms:.1f} ms")
 
 
 RENDER = {
@@ -209,7 +249,7 @@ def render(name, flags, rounds=3):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", list(RENDER))
-@pytest.mark.parametrize("extra", [0, A.PHX_F_BINARY_BVH])
+@pytest.mark.parametrize("extra", [0, A.PHX_F_BINARY_BVH, A.PHX_F_QUANT_BVH])
 def test_device_tree_renders_identically(name, extra):
     rad_h, flux_h, ih = render(name, extra)
     rad_d, flux_d, idv = render(name, extra | A.PHX_F_DEVICE_BVH)
@@ -218,6 +258,17 @@ def test_device_tree_renders_identically(name, extra):
     assert np.array_equal(rad_d.view(np.uint32), rad_h.view(np.uint32))
     assert np.array_equal(flux_d.view(np.uint32), flux_h.view(np.uint32))
     assert idv.bvh_build_ms > 0.0 and idv.setup_ms >= idv.bvh_build_ms
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(RENDER))
+def test_quantized_nodes_render_identically(name):
+    """8-bit child boxes only prune less tightly: every image equals the float-box render."""
+    rad_h, flux_h, ih = render(name, 0)
+    rad_q, flux_q, iq = render(name, A.PHX_F_QUANT_BVH)
+    assert iq.stack_overflows == 0
+    assert np.array_equal(rad_q.view(np.uint32), rad_h.view(np.uint32))
+    assert np.array_equal(flux_q.view(np.uint32), flux_h.view(np.uint32))
 
 
 @pytest.mark.gpu
