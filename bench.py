@@ -235,8 +235,8 @@ def run_ours(a, cfg: dict) -> dict | None:
         args.flags = args.flags | 4  # PHX_F_BINARY_BVH
     if a.quant_bvh:
         args.flags = args.flags | 16  # PHX_F_QUANT_BVH
-    if a.device_bvh:
-        args.flags = args.flags | 8  # PHX_F_DEVICE_BVH
+    if a.host_bvh:
+        args.flags = args.flags | 32  # PHX_F_HOST_BVH
     if a.leaf_size:
         args.bvh_leaf_size = a.leaf_size
     scene = P.SceneData.generate(cfg["kind"], seed=1, width=args.width, height=args.height, detail=cfg["detail"])
@@ -481,6 +481,10 @@ def time_to_rmse_batch16(a) -> dict:
     t_plain_conv = sum(plain[i][0] for i in conv)
     t_batch_conv = R.time_batched_schedule([specs[i] for i in conv], [r_star[i] for i in conv],
                                            pipeline=TTR_PIPELINE) if conv else None
+    # the reference's kernel shapes in the plain form, end to end, on the converging scenes
+    ref_conv = [R.time_plain_run(specs[i], r_star[i], reference_shaped=True) for i in conv]
+    t_ref_conv = sum(dt for dt, _ in ref_conv)
+    same_img = all(np.array_equal(img, plain[i][1]) for (_, img), i in zip(ref_conv, conv))
     # the reference's kernel shapes (one thread per item, its median-split tree, NEE inline), per
     # round on a 20-round sample of each scene: a secondary, extrapolated comparison
     t_ref_shape = sum(r * R.time_plain(s, 20, reference_shaped=True) for s, r in zip(specs, r_eff))
@@ -499,6 +503,9 @@ def time_to_rmse_batch16(a) -> dict:
             "converging_plain_s": round(t_plain_conv, 3),
             "converging_graph_batched_s": round(t_batch_conv, 3) if t_batch_conv else None,
             "converging_speedup": round(t_plain_conv / t_batch_conv, 3) if t_batch_conv else None,
+            "converging_plain_reference_shaped_s": round(t_ref_conv, 3),
+            "converging_speedup_vs_reference_shaped": round(t_ref_conv / t_batch_conv, 3) if t_batch_conv else None,
+            "reference_shaped_images_identical": same_img,
             "plain_reference_shaped_s_extrapolated": round(t_ref_shape, 2),
             "speedup_vs_reference_shaped": round(t_ref_shape / t_batch, 2)}
 
@@ -648,7 +655,7 @@ def scene_setup_times() -> dict:
                     np.array_equal(host.trirec.view(np.uint32), dev.trirec.view(np.uint32)))
         row = {"triangles": scene.n_triangles, "traversal_tree_host_ms": round(host.build_ms, 2),
                "traversal_tree_gpu_ms": round(dev.build_ms, 2), "identical": same}
-        for tag, flags in (("host", 0), ("gpu", A.PHX_F_DEVICE_BVH)):
+        for tag, flags in (("host", A.PHX_F_HOST_BVH), ("gpu", 0)):
             args = P.ArgsList(width=w, height=h, photons_per_round=1 << 16, flags=flags)
             with P.Renderer(args) as r:
                 r.set_scene(scene)
@@ -674,7 +681,7 @@ def main() -> int:
     ap.add_argument("--persistent", action="store_true", help="lane-refill state-machine kernels")
     ap.add_argument("--binary-bvh", action="store_true", help="traverse child pairs instead of 4-wide nodes")
     ap.add_argument("--quant-bvh", action="store_true", help="4-wide nodes with 8-bit child boxes")
-    ap.add_argument("--device-bvh", action="store_true", help="build the traversal tree on the GPU")
+    ap.add_argument("--host-bvh", action="store_true", help="build the traversal tree on the host")
     ap.add_argument("--leaf-size", type=int, default=0, help="triangles per leaf of the traversal tree (0: library default)")
     ap.add_argument("--autotune", action="store_true", help="run the library autotuner before timing")
     ap.add_argument("--shard", action="store_true",

@@ -164,9 +164,10 @@ typedef struct phx_params {
 #define PHX_F_REFERENCE_BVH 2u    /* traverse the reference's median-split tree instead of the SAH tree */
 #define PHX_F_BINARY_BVH 4u       /* traverse the SAH tree as child pairs instead of 4-wide nodes */
 #define PHX_F_QUANT_BVH 16u       /* 4-wide nodes with 8-bit child boxes (64 instead of 112 bytes) */
-#define PHX_F_DEVICE_BVH 8u       /* build the SAH traversal tree on the GPU (the same tree, bit for
-                                     bit; the reference tree for tie-break ranks is built on the host
-                                     meanwhile) */
+#define PHX_F_DEVICE_BVH 8u       /* build the SAH traversal tree on the GPU: the default (the same
+                                     tree as the host build, bit for bit; the reference tree for the
+                                     tie-break ranks is built on host threads meanwhile) */
+#define PHX_F_HOST_BVH 32u        /* build the SAH traversal tree on the host instead */
 
 /* Counters and sizes of a context. */
 typedef struct phx_info {

@@ -25,7 +25,7 @@ PHX_NO_TEXTURE = 0xFFFFFFFF
 PHX_LIGHT_POINT, PHX_LIGHT_SPOT, PHX_LIGHT_DIRECTIONAL, PHX_LIGHT_TEXTURED = range(4)
 PHX_SCENE_CORNELL, PHX_SCENE_CAUSTIC, PHX_SCENE_ATRIUM = range(3)
 PHX_F_DEFAULT, PHX_F_SIMPLE_TRAVERSAL, PHX_F_REFERENCE_BVH, PHX_F_BINARY_BVH, PHX_F_DEVICE_BVH = 0, 1, 2, 4, 8
-PHX_F_QUANT_BVH = 16
+PHX_F_QUANT_BVH, PHX_F_HOST_BVH = 16, 32
 
 BUFFERS = ["HP_POS", "HP_NORMAL", "HP_THROUGHPUT", "HP_BASE_COLOR", "HP_DIRECT", "HP_EMISSION", "FLUX",
            "PHOTON_WEIGHT", "RADIANCE", "PHOTON_POS", "PHOTON_POWER", "PHOTON_DIR", "PHOTON_HASH", "CELL_COUNT",

@@ -257,7 +257,7 @@ int Engine::upload_scene(uint32_t i, const phx_scene &s, const phx_params &p, ui
     int r;
     int32_t trav_root = 0;
     bool wide = false, trav_done = false, ref_built = false, force_ref = false;
-    if ((p.flags & PHX_F_DEVICE_BVH) && !(p.flags & PHX_F_REFERENCE_BVH) &&
+    if (!(p.flags & PHX_F_HOST_BVH) && !(p.flags & PHX_F_REFERENCE_BVH) &&
         (r = device_traversal(S, s, p, st, ref_built, trav_done, force_ref, trav_root, wide)))
         return r;
     const bool quant_req = (p.flags & PHX_F_QUANT_BVH) != 0;

@@ -239,12 +239,21 @@ def batch_images(specs, rounds: int, seed_offset: int = 0, device: int = 0,
     return imgs
 
 
-def time_plain_run(spec: SceneSpec, rounds: int, device: int = 0) -> tuple[float, np.ndarray]:
+def time_plain_run(spec: SceneSpec, rounds: int, device: int = 0,
+                   reference_shaped: bool = False) -> tuple[float, np.ndarray]:
     """Wall seconds of `rounds` rounds of one scene in the plain per-pass form (per-pass launches and
     the reference's two host syncs per round, renderer.cpp:64-86), end to end from a fresh SPPM
-    state with the scene set up beforehand, and the image it reaches."""
-    r = Renderer(spec.args(), device=device)
+    state with the scene set up beforehand, and the image it reaches.  With `reference_shaped`, the
+    kernels also take the reference's shape (see time_plain); the image is the same."""
+    args = spec.args()
+    if reference_shaped:
+        args.flags = A.PHX_F_SIMPLE_TRAVERSAL | A.PHX_F_REFERENCE_BVH
+    r = Renderer(args, device=device)
     r.set_scene(spec.scene())
+    if reference_shaped:
+        t = r.tuning()
+        t.persistent, t.nee_wavefront = 0, 0
+        r.set_tuning(t)
     r.sync()
     t0 = time.perf_counter()
     for _ in range(rounds):

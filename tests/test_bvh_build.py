@@ -1,5 +1,6 @@
-"""The traversal tree: the host builder's tree is valid (CPU), and the GPU builder returns the same
-arrays bit for bit and renders the same images (PHX_F_DEVICE_BVH, needs a GPU).
+"""The traversal tree: the host builder's tree is valid (CPU), and the GPU builder (the default;
+PHX_F_HOST_BVH selects the host one) returns the same arrays bit for bit and renders the same
+images (needs a GPU).
 
 The SAH tree is the kernels' own structure (the reference traverses the median-split tree of
 src/renderer/bvh.cpp); what it must preserve is the reference's hit for every ray, which the
@@ -251,8 +252,8 @@ def render(name, flags, rounds=3):
 @pytest.mark.parametrize("name", list(RENDER))
 @pytest.mark.parametrize("extra", [0, A.PHX_F_BINARY_BVH, A.PHX_F_QUANT_BVH])
 def test_device_tree_renders_identically(name, extra):
-    rad_h, flux_h, ih = render(name, extra)
-    rad_d, flux_d, idv = render(name, extra | A.PHX_F_DEVICE_BVH)
+    rad_h, flux_h, ih = render(name, extra | A.PHX_F_HOST_BVH)
+    rad_d, flux_d, idv = render(name, extra)
     assert (idv.trav_depth, idv.trav_inner_nodes) == (ih.trav_depth, ih.trav_inner_nodes)
     assert idv.stack_overflows == ih.stack_overflows == 0
     assert np.array_equal(rad_d.view(np.uint32), rad_h.view(np.uint32))
@@ -265,7 +266,7 @@ def test_device_tree_renders_identically(name, extra):
 def test_quantized_nodes_render_identically(name):
     """8-bit child boxes only prune less tightly: every image equals the float-box render."""
     rad_h, flux_h, ih = render(name, 0)
-    rad_q, flux_q, iq = render(name, A.PHX_F_QUANT_BVH)
+    rad_q, flux_q, iq = render(name, A.PHX_F_QUANT_BVH | A.PHX_F_HOST_BVH)
     assert iq.stack_overflows == 0
     assert np.array_equal(rad_q.view(np.uint32), rad_h.view(np.uint32))
     assert np.array_equal(flux_q.view(np.uint32), flux_h.view(np.uint32))
@@ -275,7 +276,7 @@ def test_quantized_nodes_render_identically(name):
 def test_device_tree_in_a_batch():
     specs = [("cornell", 0), ("caustic", 0), ("atrium", 0)]
     out = {}
-    for flags in (0, A.PHX_F_DEVICE_BVH):
+    for flags in (A.PHX_F_HOST_BVH, 0):
         scenes, args = [], []
         for name, _ in specs:
             kind, detail, w, h, ph, mb, g = RENDER[name]
@@ -286,5 +287,5 @@ def test_device_tree_in_a_batch():
         b.iterate(2)
         out[flags] = [b.read(i, "RADIANCE") for i in range(len(specs))]
         b.close()
-    for a, d in zip(out[0], out[A.PHX_F_DEVICE_BVH]):
+    for a, d in zip(out[A.PHX_F_HOST_BVH], out[0]):
         assert np.array_equal(a.view(np.uint32), d.view(np.uint32))
