@@ -179,7 +179,8 @@ TAIL_CONCURRENT = 2  # active scenes at or below which the camera and photon pas
 PIPELINE_ROUNDS = 8
 
 
-def time_batched_schedule(specs, r_star: list[int], device: int = 0, pipeline: int = PIPELINE_ROUNDS) -> float:
+def time_batched_schedule(specs, r_star: list[int], device: int = 0, pipeline: int = PIPELINE_ROUNDS,
+                          autotune: bool = False, info: dict | None = None) -> float:
     """Wall seconds for the batch in the graph form to give every scene its own number of rounds:
     rounds run for all active scenes, and each scene is retired as soon as it has had r_star[s].
     Once TAIL_CONCURRENT or fewer scenes remain, a round is bound by the latency of their paths and
@@ -189,6 +190,12 @@ def time_batched_schedule(specs, r_star: list[int], device: int = 0, pipeline: i
     rounds and overlaps their camera and photon passes (the gathers stay in order), which shortens
     the latency-bound rounds of few remaining scenes.  Results are bit-identical either way."""
     b = Batch([s.scene() for s in specs], [s.args() for s in specs], device=device)
+    if autotune:  # the library's autotuner on this batch, before the timed region (state restored)
+        ta = time.perf_counter()
+        chosen = b.autotune()
+        if info is not None:
+            info["autotune_s"] = time.perf_counter() - ta
+            info["tuning"] = {f: getattr(chosen, f) for f, _ in chosen._fields_ if f != "reserved"}
     order = sorted(set(r_star))
     done = 0
     active = len(specs)
