@@ -510,6 +510,27 @@ def time_to_rmse_batch16(a) -> dict:
             "speedup_vs_reference_shaped": round(t_ref_shape / t_batch, 2)}
 
 
+def time_to_rmse_full_size() -> dict:
+    """The timing half of the full-size study, short enough for the default run: the scenes of the
+    uneven batch that reach RMSE 0.01, each given its rounds to target as the full study measured
+    them (rmse.UNEVEN_ROUNDS_TO_TARGET; `--config ttr16` re-derives them with its references), in the
+    plain per-pass form one scene at a time and in the graph + batched form (autotuned first, each
+    scene retired at its count), both end to end; the stalled scenes reach the target in no form."""
+    from phosphor_b200 import rmse as R
+    specs = R.uneven_batch_specs()
+    conv = [i for i, r in enumerate(R.UNEVEN_ROUNDS_TO_TARGET) if r is not None]
+    rounds = [R.UNEVEN_ROUNDS_TO_TARGET[i] for i in conv]
+    plain = [R.time_plain_run(specs[i], r)[0] for i, r in zip(conv, rounds)]
+    info: dict = {}
+    t_batch = R.time_batched_schedule([specs[i] for i in conv], rounds, pipeline=TTR_PIPELINE, autotune=True,
+                                      info=info)
+    return {"workload": "the uneven batch's scenes that reach RMSE 0.01 (256^2..1024^2 px, 2^16..2^21 photons)",
+            "scenes": conv, "rounds_to_target": rounds, "plain_s": round(sum(plain), 3),
+            "plain_s_per_scene": [round(t, 3) for t in plain], "graph_batched_s": round(t_batch, 3),
+            "speedup": round(sum(plain) / t_batch, 3), "autotune_s": round(info.get("autotune_s", 0.0), 2),
+            "stalled_scenes": [i for i, r in enumerate(R.UNEVEN_ROUNDS_TO_TARGET) if r is None]}
+
+
 def time_to_rmse_small(a) -> dict | None:
     """The small-scene study (16 uneven scenes of 32..64 px, 2^14..2^16 photons, converged FP64
     oracle references committed in tests/golden/rmse_refs.npz): rounds to RMSE <= 0.01, and the
@@ -729,6 +750,8 @@ def main() -> int:
     if out is not None:
         if not a.no_rmse and out["n_gpus"] == 1 and a.scale == 1:
             out["time_to_rmse"] = time_to_rmse_small(a)
+        if not a.no_rmse and out["n_gpus"] == 1 and a.scale == 1:
+            out["time_to_rmse_full_size"] = time_to_rmse_full_size()
         if not a.no_setup and out["n_gpus"] == 1 and a.scale == 1:
             out["scene_setup"] = scene_setup_times()
         if not a.no_inverse and out["n_gpus"] == 1 and a.scale == 1:
