@@ -46,7 +46,7 @@ constexpr float BBOX_EPS = 1e-3f;  // bounding_box.h expansion
 constexpr float BOX_INF = 1e9f;    // bounding_box.h "infinite" coordinate
 constexpr float BIG = 1e30f;       // the host builder's empty-box bounds
 
-enum : u32 { ERR_DEGENERATE = 1u, ERR_RANGE = 2u, ERR_LEVELS = 4u };
+enum : u32 { ERR_DEGENERATE = 1u, ERR_RANGE = 2u };
 
 // order-preserving int image of a float (for atomicMin / atomicMax; -0 never occurs here)
 PHX_DI int f2o(float f) {
@@ -256,19 +256,21 @@ PHX_DI bool goes_left(const Prim &p, u32 pos, int bax, int bbin, int nb, float c
 
 // ---- one task per group of G threads (a warp, or a whole block) ----------------------------
 
+// Shared state of one group.  A warp's tasks hold at most TINY (< NB_SWITCH) triangles, so they bin
+// with NB_SMALL bins per axis; a block's may need NB_LARGE.
 template <int G> struct GroupSmem {
     static constexpr int NB = G == 32 ? NB_SMALL : NB_LARGE;
-    int bins[3 * NB * 7];
-    float ra[3][NB];
+    int bins[3 * NB * 7];   // [axis][bin]: count, lo[3], hi[3] (ordered ints)
+    float ra[3][NB];        // split search scratch: right-hand areas and counts per bin
     int rn[3][NB];
-    float red[G / 32][12];
-    float box[12];       // lo, hi, clo, chi
-    float ax_c[3];
+    float red[G / 32][12];  // per-warp bounds
+    float box[12];          // lo, hi, clo, chi of the task
+    float ax_c[3];          // best cost, bin and left count per axis
     int ax_k[3], ax_ln[3];
-    int dec[4];          // leaf?, bax, bbin, ln
-    u32 node;
-    u32 wtot[G / 32];
+    u32 node;               // the inner node allocated for the task
+    u32 wtot[G / 32];       // per-warp left | valid counts of a partition tile
 };
+static_assert(TINY < NB_SWITCH, "warp tasks bin with NB_SMALL bins");
 
 template <int G> PHX_DI void gsync() {
     if (G == 32)
@@ -278,7 +280,7 @@ template <int G> PHX_DI void gsync() {
 }
 
 template <int G> PHX_DI void process_task(const Task t, const BuildArgs &A, GroupSmem<G> &sm, int tid) {
-    constexpr int NBMAX = GroupSmem<G>::NB;
+    static_assert(G == 32 || GroupSmem<G>::NB == NB_LARGE, "a block-sized group bins up to 128 per axis");
     const u32 b = t.b, e = t.e, cnt = e - b;
     const int lane = tid & 31, warp = tid >> 5;
     // 1. bounds of the boxes and of the centroids
@@ -331,7 +333,6 @@ template <int G> PHX_DI void process_task(const Task t, const BuildArgs &A, Grou
     // 2. centroid bins
     Split s{-1, 0, 0, BIG};
     if (cnt > 1) {
-        (void)NBMAX;
         for (int i = tid; i < 3 * nb; i += G) {
             int *bn = &sm.bins[i * 7];
             bn[0] = 0;
