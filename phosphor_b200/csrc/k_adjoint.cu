@@ -465,7 +465,6 @@ __global__ void __launch_bounds__(128) k_gather_adj(LaunchCtx lc, GatherBufs g, 
     const float4 T = g.hp_throughput[gpix], A = g.hp_base_color[gpix];
     const float4 pa = a * T * (A / PI); // dL/dΦ_k = w_k · pa
     const float denom = 2.0f * r_sq;
-    const float r_sq_far = r_sq * (1.0f + 9.5367431640625e-7f); // r_sq (1 + 2^-20)
     const float qx = (pos.x - grid.ox) / grid.cx, qy = (pos.y - grid.oy) / grid.cy, qz = (pos.z - grid.oz) / grid.cz;
     const u32 G = grid.g;
     constexpr float M = 1.0f / 1024.0f;
@@ -489,9 +488,6 @@ __global__ void __launch_bounds__(128) k_gather_adj(LaunchCtx lc, GatherBufs g, 
         for (u32 k = min(__ldg(&cs[hsh]), g.n_cap); k < end; k++) {
             const float4 p = __ldg(&g.s_posdir[k]);
             const float dx = pos.x - p.x, dy = pos.y - p.y, dz = pos.z - p.z, dw = pos.w - 0.0f;
-            // the forward gather's fused rejection (k_gather.cu): the same photons pass
-            if (__fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmaf_rn(dz, dz, __fmul_rn(dw, dw)))) > r_sq_far)
-                continue;
             const float dsq = ((dx * dx + dy * dy) + dz * dz) + dw * dw;
             if (!(dsq < r_sq))
                 continue;
