@@ -18,21 +18,6 @@
 
 namespace phx {
 
-// The radius test dsq < r_sq needs the reference's squared distance ((dx² + dy²) + dz²) + dw²,
-// seven separately rounded operations.  Most photons of the 27 cells lie outside the radius
-// (the sphere fills about a tenth of the cells' volume), and for them a fused form decides it in
-// four: both forms sum non-negative terms, so each is within 4 units in the last place (4u, u =
-// 2^-24) of the true value, and a fused value above r_sq·(1 + 2^-20) (rounded: at least
-// r_sq·(1 + 15u)) puts the exact one above r_sq·(1 + 7u).  Photons the filter keeps take the
-// exact test, so the set of counted photons and every value computed from them are unchanged.
-#ifndef PHX_GATHER_FILTER
-#define PHX_GATHER_FILTER 1
-#endif
-PHX_DI float dsq_fused(float dx, float dy, float dz, float dw) {
-    return __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmaf_rn(dz, dz, __fmul_rn(dw, dw))));
-}
-constexpr float DSQ_FAR = 1.0f + 9.5367431640625e-7f; // 1 + 2^-20
-
 PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
     float4 ge = g.hp_emission[gpix];
     float4 rso = g.radiance[gpix];
@@ -67,12 +52,9 @@ PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
     // hit point in cell units, for the cell-distance test below
     const float qx = (pos.x - grid.ox) / grid.cx, qy = (pos.y - grid.oy) / grid.cy, qz = (pos.z - grid.oz) / grid.cz;
     const u32 G = grid.g;
-    const float r_sq_far = r_sq * DSQ_FAR;
     // One photon's contribution, in the reference's arithmetic (photon_hash.h:84-101).
     auto add = [&](const float4 p, u32 k) {
         const float dx = pos.x - p.x, dy = pos.y - p.y, dz = pos.z - p.z, dw = pos.w - 0.0f;
-        if (PHX_GATHER_FILTER && dsq_fused(dx, dy, dz, dw) > r_sq_far)
-            return;
         const float dsq = ((dx * dx + dy * dy) + dz * dz) + dw * dw;
         if (dsq < r_sq) {
             const float4 pd = __ldg(&g.s_dir[k]); // decode_oct(p.w), decoded once per round
