@@ -554,8 +554,14 @@ __global__ void __launch_bounds__(32) k_big_decide(BigTask *big, const int *gbin
     big_bounds(t, lo, hi, clo, chi);
     for (int a = 0; a < 3; a++)
         live[a] = __fsub_rn(chi[a], clo[a]) > 0.0f;
-    const int *bins = gbins + (size_t)blockIdx.x * 3 * NB_LARGE * 7;
+    // the task's merged bins, staged in shared memory by the whole warp: the split search walks
+    // them sequentially on three lanes, which from global memory took ~0.1 ms per task
+    __shared__ int bins[3 * NB_LARGE * 7];
+    const int *gb = gbins + (size_t)blockIdx.x * 3 * NB_LARGE * 7;
     const int tid = threadIdx.x;
+    for (int i = tid; i < 3 * NB_LARGE * 7; i += 32)
+        bins[i] = __ldcg(&gb[i]);
+    __syncwarp();
     if (tid < 3) {
         ax_k[tid] = -1;
         if (live[tid])
@@ -921,26 +927,37 @@ __global__ void k_push_root(BuildArgs A, u32 n) { push_task(A, 0, n, NO_PARENT, 
 
 u32 blocks_for(u64 n, u32 bs) { return (u32)std::max<u64>(1, (n + bs - 1) / bs); }
 
-struct Scratch { // device allocations of one build, released on every path
-    std::vector<void *> ptrs;
+// Device scratch of one build: the buffers of a layout are carved from one allocation (a build made
+// twenty cudaMalloc / cudaFree calls, each synchronising the device, before it had done any work).
+// The layout runs twice: once to size the arena, once to hand out the pointers.
+struct Scratch {
+    std::vector<void *> arenas;
+    char *base = nullptr;
+    size_t used = 0;
+    bool sizing = false;
     ~Scratch() {
-        for (void *p : ptrs)
+        for (void *p : arenas)
             cudaFree(p);
     }
     template <class T> T *get(size_t count) {
-        void *p = nullptr;
-        if (cudaMalloc(&p, std::max<size_t>(count * sizeof(T), 16)) != cudaSuccess)
-            return nullptr;
-        ptrs.push_back(p);
-        return static_cast<T *>(p);
+        const size_t off = used;
+        used += (std::max<size_t>(count * sizeof(T), 16) + 255) & ~size_t(255);
+        return sizing ? nullptr : reinterpret_cast<T *>(base + off);
     }
-};
-
-struct PinnedWords { // a few host words the level loop reads back
-    u32 *p = nullptr;
-    ~PinnedWords() {
-        if (p)
-            cudaFreeHost(p);
+    // runs layout() to size an arena, allocates it, and runs layout() again with real pointers
+    template <class F> bool carve(F &&layout) {
+        sizing = true;
+        used = 0;
+        layout();
+        void *p = nullptr;
+        if (cudaMalloc(&p, used) != cudaSuccess)
+            return false;
+        arenas.push_back(p);
+        base = static_cast<char *>(p);
+        sizing = false;
+        used = 0;
+        layout();
+        return true;
     }
 };
 
@@ -978,26 +995,40 @@ int bvh_device_build(const phx_triangle *tris, u32 n, u32 max_leaf, bool widen, 
     max_leaf = std::max(1u, std::min(max_leaf, 16u));
     Scratch S;
     const u32 big_cap = n / CHUNK + 2, chunk_cap = n / CHUNK + big_cap + 2;
-    Prim *pa = S.get<Prim>(n), *pb = S.get<Prim>(n);
-    float *rec = S.get<float>((size_t)n * 16);
-    Task *tiny[2] = {S.get<Task>(n), S.get<Task>(n)}, *med[2] = {S.get<Task>(n), S.get<Task>(n)};
-    BigTask *big[2] = {S.get<BigTask>(big_cap), S.get<BigTask>(big_cap)};
-    int *gbins = S.get<int>((size_t)big_cap * 3 * NB_LARGE * 7);
-    Chunk *chunks = S.get<Chunk>(chunk_cap);
-    u32 *chunk_left = S.get<u32>(chunk_cap);
-    Counters *ctr = S.get<Counters>(1);
-    u32 *sub = S.get<u32>(n), *pre = S.get<u32>(n);
-    PinnedWords hw;
-    if (!pa || !pb || !rec || !tiny[0] || !tiny[1] || !med[0] || !med[1] || !big[0] || !big[1] || !gbins ||
-        !chunks || !chunk_left || !ctr || !sub || !pre ||
-        cudaMalloc(&out.leaf_tri, (size_t)n * 4) != cudaSuccess ||
-        cudaMalloc(&out.leaves, (size_t)n * 8) != cudaSuccess ||
-        cudaMallocHost(&hw.p, sizeof(Counters)) != cudaSuccess) {
+    Prim *pa, *pb;
+    float *rec;
+    Task *tiny[2], *med[2];
+    BigTask *big[2];
+    int *gbins;
+    Chunk *chunks;
+    u32 *chunk_left, *sub, *pre;
+    Counters *ctr;
+    const bool carved = S.carve([&] {
+        pa = S.get<Prim>(n);
+        pb = S.get<Prim>(n);
+        rec = S.get<float>((size_t)n * 16);
+        tiny[0] = S.get<Task>(n);
+        tiny[1] = S.get<Task>(n);
+        med[0] = S.get<Task>(n);
+        med[1] = S.get<Task>(n);
+        big[0] = S.get<BigTask>(big_cap);
+        big[1] = S.get<BigTask>(big_cap);
+        gbins = S.get<int>((size_t)big_cap * 3 * NB_LARGE * 7);
+        chunks = S.get<Chunk>(chunk_cap);
+        chunk_left = S.get<u32>(chunk_cap);
+        ctr = S.get<Counters>(1);
+        sub = S.get<u32>(n);
+        pre = S.get<u32>(n);
+    });
+    if (!carved || cudaMalloc(&out.leaf_tri, (size_t)n * 4) != cudaSuccess ||
+        cudaMalloc(&out.leaves, (size_t)n * 8) != cudaSuccess) {
         out.release();
         err = "device BVH build: out of device memory";
         return 2;
     }
-    Counters *hc = reinterpret_cast<Counters *>(hw.p);
+    Counters host_ctr{};
+    Counters *hc = &host_ctr; // read back with a synchronous copy per level (a few words)
+    u32 hw[4] = {0, 0, 0, 0};
     auto fail = [&](int code, const char *msg) {
         out.release();
         err = msg;
@@ -1104,13 +1135,20 @@ int bvh_device_build(const phx_triangle *tris, u32 n, u32 max_leaf, bool widen, 
     out.wroot = out.root;
     if (widen && N > 0) {
         // the child-pair records, numbered, are the input; the wide tree has at most N nodes
-        float *wrec = S.get<float>((size_t)N * 28);
-        WTask *wt[2] = {S.get<WTask>(N), S.get<WTask>(N)};
-        u32 *wctr = S.get<u32>(4);
-        int *wroot = S.get<int>(1);
-        u32 *wsub = S.get<u32>(N), *wpre = S.get<u32>(N);
-        if (!wrec || !wt[0] || !wt[1] || !wctr || !wroot || !wsub || !wpre ||
-            cudaMalloc(&out.wnodes, (size_t)N * 28 * 4) != cudaSuccess)
+        float *wrec;
+        WTask *wt[2];
+        u32 *wctr, *wsub, *wpre;
+        int *wroot;
+        const bool wcarved = S.carve([&] {
+            wrec = S.get<float>((size_t)N * 28);
+            wt[0] = S.get<WTask>(N);
+            wt[1] = S.get<WTask>(N);
+            wctr = S.get<u32>(4);
+            wroot = S.get<int>(1);
+            wsub = S.get<u32>(N);
+            wpre = S.get<u32>(N);
+        });
+        if (!wcarved || cudaMalloc(&out.wnodes, (size_t)N * 28 * 4) != cudaSuccess)
             return fail(2, "device BVH build: out of device memory");
         const WTask root_task{0, NO_PARENT, 0u, 0u};
         cudaMemcpyAsync(wt[0], &root_task, sizeof(WTask), cudaMemcpyHostToDevice, st);
@@ -1122,12 +1160,12 @@ int bvh_device_build(const phx_triangle *tris, u32 n, u32 max_leaf, bool widen, 
             cudaMemsetAsync(wctr, 0, 4, st);
             k_widen_level<<<blocks_for(ncur, 128), 128, 0, st>>>(out.cnodes, wt[c], ncur, wrec, wt[c ^ 1], wctr,
                                                                wroot, N);
-            if ((r = sync_read(hw.p, wctr, 12, st, err)))
+            if ((r = sync_read(hw, wctr, 12, st, err)))
                 return out.release(), r;
-            if (hw.p[2])
+            if (hw[2])
                 return fail(3, "device BVH build: 4-wide collapse overflow");
-            wlevel.push_back(hw.p[1]);
-            ncur = hw.p[0];
+            wlevel.push_back(hw[1]);
+            ncur = hw[0];
             c ^= 1;
             wl++;
         }
@@ -1145,9 +1183,9 @@ int bvh_device_build(const phx_triangle *tris, u32 n, u32 max_leaf, bool widen, 
                 k_wpreorder<<<blocks_for(hi - lo, 256), 256, 0, st>>>(wrec, lo, hi, wsub, wpre);
         }
         k_wremap<<<blocks_for(W, 256), 256, 0, st>>>(wrec, W, wpre, out.wnodes, &wctr[2]);
-        if ((r = sync_read(hw.p, wctr, 12, st, err)))
+        if ((r = sync_read(hw, wctr, 12, st, err)))
             return out.release(), r;
-        if (hw.p[2])
+        if (hw[2])
             return fail(3, "device BVH build: 4-wide numbering inconsistent");
         out.n_wide = W;
         out.wdepth = wl ? wl - 1 : 0;
