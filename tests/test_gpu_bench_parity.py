@@ -62,7 +62,7 @@ def test_bench_workload_replay_equals_the_oracle(config):
     same("photon weight", got["PHOTON_WEIGHT"], st["weight"])
     same("radiance", got["RADIANCE"], st["radiance"])
     seed2 = round_seeds(args.seed, 2)[1]
-    same("hit points (round 2)", hp, o.trace(args.width, args.height, seed2, args.direct_samples))
+    same("hit points (second SPPM round)", hp, o.trace(args.width, args.height, seed2, args.direct_samples))
     counts, pos, power, dirs = o.emit(0, args.photons_per_round, args.max_photon_bounces, seed2)
     assert inf.n_photons == len(pos) == st["n_last"]
     same("per-path photon counts", got["EMIT_COUNT"], counts)
