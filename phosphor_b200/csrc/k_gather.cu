@@ -16,6 +16,12 @@
 #define PHX_GATHER_AHEAD 4
 #endif
 
+// Each cell's photon range loaded while the previous cell's photons are summed (1), or after
+// (0: one more dependent load round trip per searched cell).
+#ifndef PHX_GATHER_NEXT_CELL
+#define PHX_GATHER_NEXT_CELL 1
+#endif
+
 namespace phx {
 
 PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
@@ -71,7 +77,9 @@ PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
     // of a cell on every side so that rounding in get_hash (which decides a photon's cell) and in
     // this test can never skip a photon that would count.
     constexpr float M = 1.0f / 1024.0f;
-    for (u32 i = 0; i < 27; i++) {
+    // cell hash of neighbour offset i (0 outside the grid), and whether its box can hold a photon
+    // within the radius
+    auto cell_of = [&](u32 i, bool *near) -> u32 {
         const i32 ox = (i32)(i % 3) - 1;
         const i32 oy = (i32)((i / 3) % 3) - 1;
         const i32 oz = (i32)((i / 9) % 3) - 1;
@@ -80,16 +88,18 @@ PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
         py += (float)oy * grid.cy;
         pz += (float)oz * grid.cz;
         const u32 h = get_hash(px, py, pz, grid);
-        if (h == 0)
-            continue;
+        if (h == 0) {
+            *near = false;
+            return 0;
+        }
         const u32 hz = (h - 1) % G, hy = ((h - 1) / G) % G, hx = (h - 1) / (G * G);
         const float gx = fmaxf(fmaxf(((float)hx - M) - qx, qx - ((float)hx + (1.0f + M))), 0.0f) * grid.cx;
         const float gy = fmaxf(fmaxf(((float)hy - M) - qy, qy - ((float)hy + (1.0f + M))), 0.0f) * grid.cy;
         const float gz = fmaxf(fmaxf(((float)hz - M) - qz, qz - ((float)hz + (1.0f + M))), 0.0f) * grid.cz;
-        if ((gx * gx + gy * gy) + gz * gz > r_sq)
-            continue;
-        u32 k = min(__ldg(&cs[h]), g.n_cap);
-        const u32 end = min(__ldg(&cs[h + 1]), g.n_cap);
+        *near = !((gx * gx + gy * gy) + gz * gz > r_sq);
+        return h;
+    };
+    auto cell_photons = [&](u32 k, const u32 end) {
         // PHX_GATHER_AHEAD records in flight per step; contributions still added in photon order
 #if PHX_GATHER_AHEAD == 4
         for (; k + 3 < end; k += 4) {
@@ -111,7 +121,45 @@ PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
         }
         if (k < end)
             add(__ldg(&g.s_posdir[k]), k);
+    };
+#if PHX_GATHER_NEXT_CELL
+    // The cells to search first (arithmetic only), then each cell's photon range loaded while the
+    // previous cell's photons are summed: one dependent round trip fewer per cell.
+    u32 todo = 0;
+    for (u32 i = 0; i < 27; i++) {
+        bool near;
+        cell_of(i, &near);
+        todo |= near ? (1u << i) : 0u;
     }
+    u32 k0 = 0, k1 = 0;
+    if (todo) {
+        bool near;
+        const u32 h = cell_of(__ffs(todo) - 1, &near);
+        k0 = __ldg(&cs[h]);
+        k1 = __ldg(&cs[h + 1]);
+    }
+    while (todo) {
+        todo &= todo - 1; // the cell being summed leaves the set
+        u32 n0 = 0, n1 = 0;
+        if (todo) {
+            bool near;
+            const u32 h = cell_of(__ffs(todo) - 1, &near);
+            n0 = __ldg(&cs[h]);
+            n1 = __ldg(&cs[h + 1]);
+        }
+        cell_photons(min(k0, g.n_cap), min(k1, g.n_cap));
+        k0 = n0;
+        k1 = n1;
+    }
+#else
+    for (u32 i = 0; i < 27; i++) {
+        bool near;
+        const u32 h = cell_of(i, &near);
+        if (!near)
+            continue;
+        cell_photons(min(__ldg(&cs[h]), g.n_cap), min(__ldg(&cs[h + 1]), g.n_cap));
+    }
+#endif
     if (g.rec_r2) {
         g.rec_r2[gpix] = r_sq;
         g.rec_ratio[gpix] = found > 0.0f ? (wso + sc.alpha * found) / (wso + found) : 1.0f;
