@@ -304,9 +304,18 @@ def run_ours(a, cfg: dict) -> dict | None:
     roofline = {"bound": "hbm", "kernel": dom, "kernels": STAGE_MAP[dom], "achieved": round(achieved, 2),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 5), "traffic": traffic,
                 "peak_source": peak_kind, "per_stage": per_stage}
-    # traversal rates of the dominant kernels (not HBM bound)
+    # the whole iteration against the same peak: all stages' compulsory bytes over the iteration
+    it_bytes = sum(algo.values())
+    roofline["iteration"] = {"algo_bytes": it_bytes, "ms": round(ms / a.steps, 4),
+                             "gbs": round(it_bytes / (ms / a.steps * 1e-3) / 1e9, 1),
+                             "frac": round(it_bytes / (ms / a.steps * 1e-3) / 1e9 / peak, 5)}
+    # traversal rates of the dominant kernels (not HBM bound): camera paths, shadow rays (every
+    # diffuse hit point's direct_samples rays plus the deferred specular samples), photon paths
+    hit = int((r.read("HP_EMISSION")[:, 3] == 1.0).sum())
+    shadow_rays = hit * args.direct_samples + info.spec_samples
     rays = {"camera_paths_per_s": Pn / (stages["trace"] * 1e-3), "photon_paths_per_s":
-            args.photons_per_round / (stages["emit"] * 1e-3)}
+            args.photons_per_round / (stages["emit"] * 1e-3), "shadow_rays_per_round": shadow_rays,
+            "shadow_rays_per_s": shadow_rays / (stages["shadow"] * 1e-3)}
 
     # end to end through the public API: host seed in (pinned H2D), one round, 8-bit image out
     host_rng = [0]

@@ -123,31 +123,33 @@ PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
             add(__ldg(&g.s_posdir[k]), k);
     };
 #if PHX_GATHER_NEXT_CELL
-    // The cells to search first (arithmetic only), then each cell's photon range loaded while the
-    // previous cell's photons are summed: one dependent round trip fewer per cell.
-    u32 todo = 0;
-    for (u32 i = 0; i < 27; i++) {
-        bool near;
-        cell_of(i, &near);
-        todo |= near ? (1u << i) : 0u;
-    }
+    // Each cell's photon range is loaded while the previous cell's photons are summed: the scan for
+    // the next cell to search (each neighbour's hash computed once, as before) runs ahead by one.
+    auto next_cell = [&](u32 from, u32 *h) -> u32 {
+        for (u32 c = from; c < 27; c++) {
+            bool near;
+            *h = cell_of(c, &near);
+            if (near)
+                return c;
+        }
+        return 27u;
+    };
+    u32 h = 0;
+    u32 i = next_cell(0, &h);
     u32 k0 = 0, k1 = 0;
-    if (todo) {
-        bool near;
-        const u32 h = cell_of(__ffs(todo) - 1, &near);
+    if (i < 27) {
         k0 = __ldg(&cs[h]);
         k1 = __ldg(&cs[h + 1]);
     }
-    while (todo) {
-        todo &= todo - 1; // the cell being summed leaves the set
-        u32 n0 = 0, n1 = 0;
-        if (todo) {
-            bool near;
-            const u32 h = cell_of(__ffs(todo) - 1, &near);
-            n0 = __ldg(&cs[h]);
-            n1 = __ldg(&cs[h + 1]);
+    while (i < 27) {
+        u32 hn = 0, n0 = 0, n1 = 0;
+        const u32 j = next_cell(i + 1, &hn);
+        if (j < 27) {
+            n0 = __ldg(&cs[hn]);
+            n1 = __ldg(&cs[hn + 1]);
         }
         cell_photons(min(k0, g.n_cap), min(k1, g.n_cap));
+        i = j;
         k0 = n0;
         k1 = n1;
     }
