@@ -45,17 +45,25 @@ def _headers_mtime() -> float:
     return max((h.stat().st_mtime for h in hs), default=0.0)
 
 
+def _tmp_path(target: Path) -> Path:
+    """A file beside `target` private to this process: builds racing in parallel test workers
+    each link into their own file and the last rename wins."""
+    return target.with_name(f".{target.name}.{os.getpid()}.tmp")
+
+
 def _compile(src: Path, force: bool, hdr_mtime: float) -> Path:
     obj = BUILD / (src.name + ".o")
     if not force and obj.exists() and obj.stat().st_mtime >= max(src.stat().st_mtime, hdr_mtime):
         return obj
+    tmp = _tmp_path(obj)
     if src.suffix == ".cu":
-        cmd = [NVCC, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+        cmd = [NVCC, *NVCC_FLAGS, "-c", str(src), "-o", str(tmp)]
     else:
-        cmd = ["g++", *CXX_FLAGS, "-c", str(src), "-o", str(obj)]
+        cmd = ["g++", *CXX_FLAGS, "-c", str(src), "-o", str(tmp)]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"compile failed: {src.name}\n{' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
+    os.replace(tmp, obj)
     return obj
 
 
@@ -67,7 +75,7 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
         objs = list(ex.map(lambda s: _compile(s, force, hm), srcs))
     newest = max(o.stat().st_mtime for o in objs)
     if force or not LIB.exists() or LIB.stat().st_mtime < newest:
-        tmp = LIB.with_suffix(".so.tmp")
+        tmp = _tmp_path(LIB)
         cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs), "-lpthread", "-ldl", "-lrt", "-lz"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
@@ -88,7 +96,7 @@ def build_cli(force: bool = False, verbose: bool = False) -> Path:
     deps = srcs + [HOST_DIR / "renderer.hpp", INCLUDE / "phx.h", LIB]
     if not force and CLI.exists() and CLI.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
         return CLI
-    tmp = CLI.with_suffix(".tmp")
+    tmp = _tmp_path(CLI)
     cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-I", str(INCLUDE), "-o", str(tmp), *map(str, srcs),
            f"-L{PKG}", "-lphx", "-Wl,-rpath,$ORIGIN", "-lpthread"]
     res = subprocess.run(cmd, capture_output=True, text=True)
@@ -109,7 +117,7 @@ def build_oracle(force: bool = False, verbose: bool = False) -> Path:
                    INCLUDE / "phx_math.h", CSRC / "host.hpp"]
     if not force and ORACLE_LIB.exists() and ORACLE_LIB.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
         return ORACLE_LIB
-    tmp = ORACLE_LIB.with_suffix(".so.tmp")
+    tmp = _tmp_path(ORACLE_LIB)
     cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fvisibility=hidden", "-ffp-contract=off",
            "-I", str(INCLUDE), "-o", str(tmp), *map(str, srcs), "-lpthread"]
     res = subprocess.run(cmd, capture_output=True, text=True)
