@@ -583,14 +583,19 @@ PHX_SHADE_NEE bool sample_light_fragment(Rng *rng, const SceneDesc &sc, float4 p
 // light_sampling.h:302-333
 // A shadow ray crossing the surface it hit at h (one step of the walk in shadow_transmittance):
 // false when the surface blocks the ray (the transmittance is then zero).
-PHX_DI bool shadow_cross(const SceneDesc &sc, const Hit &h, float4 origin, float4 dir, float t_min, float4 *trans) {
+// uv_pending: h carries no barycentrics yet (a hit taken from a HitList without them).
+PHX_DI bool shadow_cross(const SceneDesc &sc, const Hit &h, float4 origin, float4 dir, float t_min, float4 *trans,
+                         bool uv_pending = false) {
     u32 mi = tri_mat(sc, h.tri);
     const phx_material &mat = sc.materials[mi];
     if (mat.transmission < EPS)
         return false;
     float4 base = f4(mat.base_color);
     if (mat.diff_index != NO_TEXTURE) {
-        SurfaceHit s = process_hit(sc, h, origin, dir);
+        Hit hh = h;
+        if (uv_pending)
+            hit_uv(sc, h.tri, origin, dir, &hh.u, &hh.v);
+        SurfaceHit s = process_hit(sc, hh, origin, dir);
         base *= srgb_to_linear(sample_texture_uv(sc, mi, mat.diff_index, s.uvx, s.uvy, 0));
     }
     float4 tr = *trans;
@@ -651,8 +656,7 @@ PHX_DI float4 shadow_transmittance(const SceneDesc &sc, float4 origin, float4 di
             for (int i = 0; i < K; i++) {
                 if (!found && i < L.n && !(L.t[i] < t_min)) {
                     h.t = L.t[i];
-                    h.u = L.u[i];
-                    h.v = L.v[i];
+                    h.u = h.v = 0.0f; // recomputed by shadow_cross where a texture needs them
                     h.tri = L.tri[i];
                     found = true;
                 }
@@ -661,7 +665,7 @@ PHX_DI float4 shadow_transmittance(const SceneDesc &sc, float4 origin, float4 di
                 break; // not vouched for: closest-hit queries from here on
             if (!found)
                 return trans; // no surface left on the segment
-            if (!shadow_cross(sc, h, origin, dir, t_min, &trans))
+            if (!shadow_cross(sc, h, origin, dir, t_min, &trans, true))
                 return zero4();
             t_min = h.t + EPS;
         }

@@ -668,6 +668,51 @@ def test_shadow_rays_through_several_transmissive_surfaces():
     assert diffuse.mean() > 0.3 and (want[diffuse, 4, :3] > 0).any()  # light reaches through the panes
 
 
+def test_shadow_rays_through_a_textured_transmissive_pane():
+    """Shadow rays crossing a transmissive surface whose base colour is a texture: the hit list of
+    the shadow traversal keeps no barycentrics, so the crossing recomputes u, v for the texture
+    lookup; hit points (direct light included) must stay bit-exact.  The scene is the textured
+    Cornell box of the reference fixture with a horizontal pane of its textured, half-transmissive
+    material between the floor and the light."""
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parent))
+    import ref_fixture as F
+    case = next(c for c in F.load_cases() if c["name"] == "cornell_textured")
+    arrays = {k[len("arr_"):]: v for k, v in case.items() if k.startswith("arr_")}
+    base = P.SceneData.generate(A.PHX_SCENE_CORNELL, seed=1, width=16, height=16)
+    dt = base.triangles().dtype
+    tris = np.frombuffer(arrays["tris"].tobytes(), dtype=dt).copy()
+    mats = np.frombuffer(arrays["mats"].tobytes(), dtype=base.materials().dtype)
+    glass = [i for i, m in enumerate(mats) if m["transmission"] > 0.0 and m["diff_index"] != 0xFFFFFFFF]
+    assert glass, "the textured fixture has a textured transmissive material"
+    pane = np.zeros(2, dtype=dt)
+    corners = [(0.1, 0.1), (0.9, 0.1), (0.9, 0.9), (0.1, 0.9)]
+    for k, tri in enumerate(((0, 1, 2), (0, 2, 3))):
+        p = pane[k]
+        for v, uv, c in zip(("v0", "v1", "v2"), ("uv0", "uv1", "uv2"), tri):
+            p[v]["x"], p[v]["y"], p[v]["z"] = corners[c][0], 0.55, corners[c][1]
+            p[uv]["x"], p[uv]["y"] = corners[c][0] * 1.7, corners[c][1] * 0.8
+        for n in ("n0", "n1", "n2"):
+            p[n]["y"] = 1.0
+        p["mat_index"] = glass[0]
+    arrays["tris"] = np.frombuffer(np.concatenate([tris, pane]).tobytes(), np.uint8).copy()
+    scene = F.ArrayScene(arrays)
+    args = P.ArgsList(width=40, height=40, photons_per_round=1 << 12, max_photon_bounces=8, grid_res=16,
+                      direct_samples=16)
+    o = O.Oracle(scene)
+    with P.Renderer(args) as r:
+        r.set_scene(scene)
+        seed = 0x7A3E
+        r.trace_rays(seed)
+        got = np.stack([r.read(b) for b in ["HP_POS", "HP_NORMAL", "HP_THROUGHPUT", "HP_BASE_COLOR", "HP_DIRECT",
+                                             "HP_EMISSION"]], axis=1)
+    want = o.trace(args.width, args.height, seed, args.direct_samples)
+    assert assert_close("textured pane hit points", got, want) == 1.0
+    below = (want[:, 5, 3] == 1.0) & (want[:, 0, 1] < 0.5)  # diffuse hit points under the pane
+    assert below.mean() > 0.1 and (want[below, 4, :3] > 0).any()  # light reaches them through it
+
+
 def test_light_samples_with_varying_draws_and_few_samples():
     """Light samples are drawn where their shadow rays are traced, each from the RNG state advanced
     past the samples before it, when every light sample takes the same number of draws.  Two other
