@@ -497,7 +497,7 @@ PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, floa
 }
 
 // Shadow kernels: general (each scene's materials decide at run time between the listing traversal
-// with its walk and the walk's any-hit query), or for contexts whose scenes have no transmissive
+// with its walk and the walk's any-hit query), for contexts whose scenes have no transmissive
 // material (a single any-hit query in slot order, and nothing else compiled in).
 enum : int { SHADOW_GENERAL = 0, SHADOW_OPAQUE = 1 };
 

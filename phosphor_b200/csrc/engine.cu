@@ -660,7 +660,8 @@ void Engine::enq_trace_r(RoundSet &R, cudaStream_t s) {
     // every sample of a hit point is one ray when the only light is a point, spot or directional one
     const bool per_pixel = sc.size() == 1 && shard.world == 1 && sc[0].lights.size() == 1 &&
                            sc[0].lights[0].kind != PHX_LIGHT_TEXTURED;
-    launch_shadow(l, o, transmissive ? SHADOW_GENERAL : SHADOW_OPAQUE, presample, per_pixel, sc[0].desc.n_pixels, s);
+    launch_shadow(l, o, transmissive ? SHADOW_GENERAL : SHADOW_OPAQUE, presample, per_pixel, sc[0].desc.n_pixels,
+                  sc.size() == 1 ? &sc[0].desc : nullptr, s);
     launch_nee_resolve(l, o, s);
     if (spec)
         launch_spec_resolve(l, o, s);
@@ -671,7 +672,8 @@ void Engine::enq_trace_r(RoundSet &R, cudaStream_t s) {
 void Engine::enq_emit_r(RoundSet &R, cudaStream_t s) {
     ev(ST_EMIT, false, s);
     EmitOut o{R.slot_pos, R.slot_pd, R.counts};
-    launch_emit(lc(R), o, (int)tune.emit_block, (int)tune.persistent, (int)tune.emit_blocks_per_sm, R.queue + 1, s);
+    launch_emit(lc(R), o, (int)tune.emit_block, (int)tune.persistent, (int)tune.emit_blocks_per_sm, R.queue + 1,
+                untextured(), s);
     ev(ST_EMIT, true, s);
     ev(ST_EMIT_SCAN, false, s);
     launch_scan(R.counts, R.offsets, (u64)total_emit + 1, R.scan_scr, R.ntotal, d_err.as<u32>(), s);
@@ -821,6 +823,16 @@ int Engine::scene_photon_range(uint32_t s, uint32_t *off, uint32_t *n) {
     *off = a;
     *n = b - a;
     return PHX_OK;
+}
+
+bool Engine::untextured() const {
+    for (const auto &s : sc)
+        for (const auto &m : s.mats)
+            if (m.diff_index != PHX_NO_TEXTURE || m.emis_index != PHX_NO_TEXTURE || m.norm_index != PHX_NO_TEXTURE ||
+                m.occlusion_index != PHX_NO_TEXTURE || m.metal_rough_index != PHX_NO_TEXTURE ||
+                m.transmission_index != PHX_NO_TEXTURE)
+                return false;
+    return true;
 }
 
 bool Engine::any_active() const {
@@ -1120,6 +1132,8 @@ int Engine::seeded_round(uint32_t seed) {
 }
 
 int Engine::upload_descs() {
+    if (sc.size() == 1)
+        invalidate_graph(); // the captured shadow launch holds the descriptor by value
     std::vector<SceneDesc> d(sc.size());
     for (size_t i = 0; i < sc.size(); i++)
         d[i] = sc[i].desc;

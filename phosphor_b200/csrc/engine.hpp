@@ -142,6 +142,7 @@ class Engine {
     int shard_nccl_init(const uint8_t *id);
     int shard_round();
     bool any_active() const;
+    bool untextured() const; // no material of any scene has a texture (indices are fixed at set-up)
 
     // differentiation (single-scene engines; engine_adjoint.cu)
     int set_materials(const phx_material *m, uint32_t n);

@@ -121,12 +121,18 @@ PHX_DI void pp_start(PhotonPath &p, const SceneDesc *sc, u32 seed, u32 tid, u32 
     p.throughput = f4(1.0f, 1.0f, 1.0f, 0.0f);
 }
 
-// Consumes the pending query; returns true while the path continues.
+// Consumes the pending query; returns true while the path continues.  NOTEX: no material of the
+// context has a texture (texture indices never change after set-up), so every texture branch is
+// compiled out of this instance.
+template <bool NOTEX>
 PHX_DI bool pp_advance(PhotonPath &p, bool hit, const Hit &h, const EmitOut &out) {
     const SceneDesc &sc = *p.sc;
     if (!hit)
         return false;
-    const phx_material mat = sc.materials[tri_mat(sc, h.tri)];
+    phx_material mat = sc.materials[tri_mat(sc, h.tri)];
+    if constexpr (NOTEX)
+        mat.diff_index = mat.emis_index = mat.norm_index = mat.occlusion_index = mat.metal_rough_index =
+            mat.transmission_index = NO_TEXTURE;
     SurfaceHit sh = process_hit(sc, h, p.origin, p.dir, mat_textured(mat));
     float cur = current_ior(&p.ior);
     if (cur != AIR_IOR && mat.thickness > EPS && mat.att_dist > EPS) {
@@ -164,6 +170,7 @@ PHX_DI bool pp_advance(PhotonPath &p, bool hit, const Hit &h, const EmitOut &out
     return p.depth < sc.max_bounces;
 }
 
+template <bool NOTEX>
 __global__ void __launch_bounds__(128, PHX_EMIT_MINB) k_emit_persistent(LaunchCtx lc, EmitOut out, u32 *queue) {
     const u32 lane = threadIdx.x & 31u;
     const u32 lt_mask = (1u << lane) - 1u;
@@ -199,7 +206,7 @@ __global__ void __launch_bounds__(128, PHX_EMIT_MINB) k_emit_persistent(LaunchCt
         if (active) {
             Hit h;
             const bool hit = intersect(*p.sc, p.origin, p.dir, EPS, INF, &h, &ovf);
-            if (!pp_advance(p, hit, h, out)) {
+            if (!pp_advance<NOTEX>(p, hit, h, out)) {
                 out.counts[p.gid] = p.n_out;
                 active = false;
             }
@@ -210,13 +217,16 @@ __global__ void __launch_bounds__(128, PHX_EMIT_MINB) k_emit_persistent(LaunchCt
 }
 
 void launch_emit(const LaunchCtx &lc, const EmitOut &out, int block, int persistent, int blocks_per_sm, u32 *queue,
-                 cudaStream_t st) {
+                 bool untextured, cudaStream_t st) {
     if (lc.emit_hi <= lc.emit_lo)
         return;
     if (persistent && queue && !out.slot_pow) {
         cudaMemsetAsync(queue, 0, sizeof(u32), st);
         int grid = g_sm_count * (blocks_per_sm > 0 ? blocks_per_sm : 8);
-        k_emit_persistent<<<grid, 128, 0, st>>>(lc, out, queue);
+        if (untextured) // emit 4.52 -> 4.44 ms (caustic), 2.82 -> 2.73 ms (atrium)
+            k_emit_persistent<true><<<grid, 128, 0, st>>>(lc, out, queue);
+        else
+            k_emit_persistent<false><<<grid, 128, 0, st>>>(lc, out, queue);
     } else {
         (void)block;
         u32 grid = (lc.emit_hi - lc.emit_lo + 127) / 128;

@@ -588,7 +588,8 @@ __global__ void __launch_bounds__(128, PHX_TRACE_MINB) k_trace_persistent(Launch
 // ---- shadow wavefront ---------------------------------------------------------------------------
 // One thread per recorded NEE sample; the ds samples of a pixel are consecutive threads, so a warp
 // traces shadow rays from one or two hit points toward the same light: coherent traversal.
-template <int KIND, bool PER_PIXEL> PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 first_block);
+template <int KIND, bool PER_PIXEL, bool ONE>
+PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 first_block, const SceneDesc &one);
 
 // Blocks [0, nee_blocks): one diffuse sample slot per thread.  Blocks from nee_blocks on (only when
 // the specular NEE is deferred): the specular sample slots, grid-stride; being last in the grid
@@ -598,18 +599,24 @@ template <int KIND, bool PER_PIXEL> PHX_DI void shadow_spec_slots(const LaunchCt
 // light is a sample's only random draw, so all ds samples of a hit point are the same ray with the
 // same weight; one thread per pixel traces sample 0 and writes its contribution to the pixel's ds
 // slots, which k_nee_resolve then sums as before (the same values in the same order).
-template <int KIND, bool PER_PIXEL>
-__global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow(LaunchCtx lc, TraceOut out, u32 nee_blocks) {
+// ONE: a single-scene context whose scene descriptor comes as a kernel parameter (`one`), so the
+// traversal reads its pointers and sizes from the constant bank instead of holding them in
+// registers (caustic shadow stage 6.80 -> 6.71 ms; the same form of the photon kernel measured no
+// gain).  A captured graph then holds the descriptor by value: the engine re-captures after any
+// change of a single scene's descriptor.
+template <int KIND, bool PER_PIXEL, bool ONE>
+__global__ void __launch_bounds__(128, PHX_SHADOW_MINB)
+    k_shadow(LaunchCtx lc, TraceOut out, u32 nee_blocks, const __grid_constant__ SceneDesc one) {
     constexpr bool per_pixel = PER_PIXEL;
     if (blockIdx.x >= nee_blocks) {
-        shadow_spec_slots<KIND, PER_PIXEL>(lc, out, nee_blocks);
+        shadow_spec_slots<KIND, PER_PIXEL, ONE>(lc, out, nee_blocks, one);
         return;
     }
     const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (per_pixel ? lc.scenes[0].n_pixels : lc.total_nee))
+    if (t >= (per_pixel ? (ONE ? one : lc.scenes[0]).n_pixels : lc.total_nee))
         return;
-    const u32 s = per_pixel || lc.n_scenes == 1 ? 0 : find_scene(lc.nee_bases, lc.n_scenes, t);
-    const SceneDesc &sc = lc.scenes[s];
+    const u32 s = per_pixel || ONE || lc.n_scenes == 1 ? 0 : find_scene(lc.nee_bases, lc.n_scenes, t);
+    const SceneDesc &sc = ONE ? one : lc.scenes[s];
     if (!sc.active)
         return;
     const u32 ds = sc.direct_samples;
@@ -660,16 +667,16 @@ __global__ void __launch_bounds__(128, PHX_SHADOW_MINB) k_shadow(LaunchCtx lc, T
 // contribution is the traced form's: weight * transmittance, zero for a sample without a ray.
 // per_pixel (see k_shadow): an event's ds samples, ds consecutive slots from a multiple of ds, are
 // one ray with one weight: one thread per event traces its first slot and fills all ds.
-template <int KIND, bool PER_PIXEL>
-PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 first_block) {
+template <int KIND, bool PER_PIXEL, bool ONE>
+PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 first_block, const SceneDesc &one) {
     const u32 n = min(*out.spec_next, out.spec_cap);
     const u32 stride = (gridDim.x - first_block) * blockDim.x;
-    const u32 step = PER_PIXEL ? lc.scenes[0].direct_samples : 1u;
+    const u32 step = PER_PIXEL ? (ONE ? one : lc.scenes[0]).direct_samples : 1u;
     u32 ovf = 0;
     for (u32 e = (blockIdx.x - first_block) * blockDim.x + threadIdx.x; (u64)e * step < n; e += stride) {
         const u32 g = e * step;
         const u32 gpix = out.spec_pix[g];
-        const SceneDesc &sc = lc.scenes[lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gpix)];
+        const SceneDesc &sc = ONE ? one : lc.scenes[lc.n_scenes == 1 ? 0 : find_scene(lc.pix_bases, lc.n_scenes, gpix)];
         const float4 hdr = out.spec_ray[g];
         float4 org, dir = zero4(), w = zero4();
         float dist = -1.0f; // < 0: no contribution
@@ -795,8 +802,17 @@ __global__ void __launch_bounds__(128) k_nee_sample(LaunchCtx lc, TraceOut out) 
     record_nee(sc, &rng, out.pos[gpix], out.stash_sn[gpix], out.base_color[gpix], out, slot);
 }
 
+template <int KIND, bool PER_PIXEL>
+static void launch_shadow_kind(const LaunchCtx &lc, const TraceOut &out, u32 grid, u32 nee_blocks, const SceneDesc *one,
+                               cudaStream_t st) {
+    if (one)
+        k_shadow<KIND, PER_PIXEL, true><<<grid, 128, 0, st>>>(lc, out, nee_blocks, *one);
+    else
+        k_shadow<KIND, PER_PIXEL, false><<<grid, 128, 0, st>>>(lc, out, nee_blocks, SceneDesc{});
+}
+
 void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int kind, bool presample, bool per_pixel,
-                   u32 n_pixels, cudaStream_t st) {
+                   u32 n_pixels, const SceneDesc *one, cudaStream_t st) {
     if (!lc.nee_defer || lc.total_nee == 0)
         return;
     if (presample && lc.pix_hi > lc.pix_lo)
@@ -805,14 +821,16 @@ void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int kind, bool pres
     const u32 nee_blocks = ((per_pixel ? n_pixels : lc.total_nee) + 127) / 128;
     const u32 spec_blocks = out.spec_ray && out.spec_cap ? (u32)g_sm_count * 8u : 0u;
     const u32 grid = nee_blocks + spec_blocks;
+    if (lc.n_scenes != 1)
+        one = nullptr;
     if (kind == SHADOW_OPAQUE && per_pixel)
-        k_shadow<SHADOW_OPAQUE, true><<<grid, 128, 0, st>>>(lc, out, nee_blocks);
+        launch_shadow_kind<SHADOW_OPAQUE, true>(lc, out, grid, nee_blocks, one, st);
     else if (kind == SHADOW_OPAQUE)
-        k_shadow<SHADOW_OPAQUE, false><<<grid, 128, 0, st>>>(lc, out, nee_blocks);
+        launch_shadow_kind<SHADOW_OPAQUE, false>(lc, out, grid, nee_blocks, one, st);
     else if (per_pixel)
-        k_shadow<SHADOW_GENERAL, true><<<grid, 128, 0, st>>>(lc, out, nee_blocks);
+        launch_shadow_kind<SHADOW_GENERAL, true>(lc, out, grid, nee_blocks, one, st);
     else
-        k_shadow<SHADOW_GENERAL, false><<<grid, 128, 0, st>>>(lc, out, nee_blocks);
+        launch_shadow_kind<SHADOW_GENERAL, false>(lc, out, grid, nee_blocks, one, st);
 }
 
 void launch_nee_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st) {

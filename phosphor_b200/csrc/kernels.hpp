@@ -64,8 +64,9 @@ void launch_trace(const LaunchCtx &lc, const TraceOut &out, int block, int persi
 // kind: SHADOW_OPAQUE when no scene has a transmissive material, else SHADOW_GENERAL.  presample:
 // some scene's light samples take varying RNG draws, so k_nee_sample draws its samples first.
 // per_pixel: a single scene whose only light is not an area light (one shadow ray per hit point)
+// one: the scene descriptor of a single-scene context (passed to the kernel by value), or null
 void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int kind, bool presample, bool per_pixel,
-                   u32 n_pixels, cudaStream_t st);
+                   u32 n_pixels, const SceneDesc *one, cudaStream_t st);
 void launch_nee_resolve(const LaunchCtx &lc, const TraceOut &out, cudaStream_t st);
 // Deferred specular NEE: complete each listed pixel's emission once k_shadow has traced the
 // claimed sample slots.
@@ -77,8 +78,9 @@ struct EmitOut {
     u32 *counts;       // per photon path (global emit index)
     float4 *slot_pow;  // optional (one-thread-per-path form only): unquantised power per slot
 };
+// untextured: no material of the context has a texture
 void launch_emit(const LaunchCtx &lc, const EmitOut &out, int block, int persistent, int blocks_per_sm, u32 *queue,
-                 cudaStream_t st);
+                 bool untextured, cudaStream_t st);
 
 // grid build
 struct GridBufs {
