@@ -498,8 +498,10 @@ PHX_DI bool intersect(const SceneDesc &sc, float4 o, float4 d, float t_min, floa
 
 // Shadow kernels: general (each scene's materials decide at run time between the listing traversal
 // with its walk and the walk's any-hit query), for contexts whose scenes have no transmissive
-// material (a single any-hit query in slot order, and nothing else compiled in).
-enum : int { SHADOW_GENERAL = 0, SHADOW_OPAQUE = 1 };
+// material (a single any-hit query in slot order, and nothing else compiled in), or general for
+// contexts with no texture at all (SHADOW_CLEAR: the textured crossing compiled out, which frees
+// most of the general kernel's spills).
+enum : int { SHADOW_GENERAL = 0, SHADOW_OPAQUE = 1, SHADOW_CLEAR = 2 };
 
 // Any-hit query of a shadow ray in a scene where no material transmits.  It visits a 4-wide node's
 // children in slot order: an unoccluded ray visits every box on its segment whatever the order,

@@ -584,6 +584,8 @@ PHX_SHADE_NEE bool sample_light_fragment(Rng *rng, const SceneDesc &sc, float4 p
 // A shadow ray crossing the surface it hit at h (one step of the walk in shadow_transmittance):
 // false when the surface blocks the ray (the transmittance is then zero).
 // uv_pending: h carries no barycentrics yet (a hit taken from a HitList without them).
+// NOTEX: no material of the context has a texture.
+template <bool NOTEX = false>
 PHX_DI bool shadow_cross(const SceneDesc &sc, const Hit &h, float4 origin, float4 dir, float t_min, float4 *trans,
                          bool uv_pending = false) {
     u32 mi = tri_mat(sc, h.tri);
@@ -591,7 +593,7 @@ PHX_DI bool shadow_cross(const SceneDesc &sc, const Hit &h, float4 origin, float
     if (mat.transmission < EPS)
         return false;
     float4 base = f4(mat.base_color);
-    if (mat.diff_index != NO_TEXTURE) {
+    if (!NOTEX && mat.diff_index != NO_TEXTURE) {
         Hit hh = h;
         if (uv_pending)
             hit_uv(sc, h.tri, origin, dir, &hh.u, &hh.v);
@@ -609,13 +611,14 @@ PHX_DI bool shadow_cross(const SceneDesc &sc, const Hit &h, float4 origin, float
 // The walk of shadow_transmittance by closest-hit queries (any-hit where no material transmits),
 // from step `depth` at t_min with the transmittance so far.  (Compiled out of line it freed the
 // shadow kernels' spills but measured 5 % slower.)
+template <bool NOTEX = false>
 PHX_DI float4 shadow_walk(const SceneDesc &sc, float4 origin, float4 dir, float t_min, float t_max, u32 depth,
                                   float4 trans, u32 *overflow) {
     for (; depth < MAX_RAY_BOUNCES; depth++) {
         Hit h;
         if (!intersect(sc, origin, dir, t_min, t_max, &h, overflow, sc.any_transmissive == 0))
             break;
-        if (!shadow_cross(sc, h, origin, dir, t_min, &trans))
+        if (!shadow_cross<NOTEX>(sc, h, origin, dir, t_min, &trans))
             return zero4();
         t_min = h.t + EPS;
     }
@@ -665,13 +668,13 @@ PHX_DI float4 shadow_transmittance(const SceneDesc &sc, float4 origin, float4 di
                 break; // not vouched for: closest-hit queries from here on
             if (!found)
                 return trans; // no surface left on the segment
-            if (!shadow_cross(sc, h, origin, dir, t_min, &trans, true))
+            if (!shadow_cross<KIND == SHADOW_CLEAR>(sc, h, origin, dir, t_min, &trans, true))
                 return zero4();
             t_min = h.t + EPS;
         }
     }
 #endif
-    return shadow_walk(sc, origin, dir, t_min, t_max, depth, trans, overflow);
+    return shadow_walk<KIND == SHADOW_CLEAR>(sc, origin, dir, t_min, t_max, depth, trans, overflow);
     }
 }
 

@@ -660,7 +660,8 @@ void Engine::enq_trace_r(RoundSet &R, cudaStream_t s) {
     // every sample of a hit point is one ray when the only light is a point, spot or directional one
     const bool per_pixel = sc.size() == 1 && shard.world == 1 && sc[0].lights.size() == 1 &&
                            sc[0].lights[0].kind != PHX_LIGHT_TEXTURED;
-    launch_shadow(l, o, transmissive ? SHADOW_GENERAL : SHADOW_OPAQUE, presample, per_pixel, sc[0].desc.n_pixels,
+    const int kind = !transmissive ? SHADOW_OPAQUE : untextured() ? SHADOW_CLEAR : SHADOW_GENERAL;
+    launch_shadow(l, o, kind, presample, per_pixel, sc[0].desc.n_pixels,
                   sc.size() == 1 ? &sc[0].desc : nullptr, s);
     launch_nee_resolve(l, o, s);
     if (spec)

@@ -79,20 +79,34 @@ PHX_DI void gather_pixel(const SceneDesc &sc, u32 gpix, const GatherBufs &g) {
     constexpr float M = 1.0f / 1024.0f;
     // cell hash of neighbour offset i (0 outside the grid), and whether its box can hold a photon
     // within the radius
+    // get_hash of a neighbour position works axis by axis, and an axis's coordinate only takes the
+    // three values pos + {-1, 0, 1} * cell: each axis's three cell coordinates are computed once,
+    // with the same operations get_hash applies (0xff: outside the grid, which has at most 255
+    // cells per axis), and packed one byte per offset.
+    const float gf = (float)G;
+    auto axis_cells = [&](float p, float o, float c) -> u32 {
+        u32 w = 0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            float q = p;
+            q += (float)(k - 1) * c;
+            const float f = (q - o) / c;
+            const u32 ci = (f < 0.0f || f >= gf) ? 0xffu : (u32)f;
+            w |= ci << (8 * k);
+        }
+        return w;
+    };
+    const u32 wx = axis_cells(pos.x, grid.ox, grid.cx), wy = axis_cells(pos.y, grid.oy, grid.cy),
+              wz = axis_cells(pos.z, grid.oz, grid.cz);
     auto cell_of = [&](u32 i, bool *near) -> u32 {
-        const i32 ox = (i32)(i % 3) - 1;
-        const i32 oy = (i32)((i / 3) % 3) - 1;
-        const i32 oz = (i32)((i / 9) % 3) - 1;
-        float px = pos.x, py = pos.y, pz = pos.z;
-        px += (float)ox * grid.cx;
-        py += (float)oy * grid.cy;
-        pz += (float)oz * grid.cz;
-        const u32 h = get_hash(px, py, pz, grid);
-        if (h == 0) {
+        const u32 hx = (wx >> (8 * (i % 3))) & 0xffu;
+        const u32 hy = (wy >> (8 * ((i / 3) % 3))) & 0xffu;
+        const u32 hz = (wz >> (8 * ((i / 9) % 3))) & 0xffu;
+        if (hx == 0xffu || hy == 0xffu || hz == 0xffu) {
             *near = false;
             return 0;
         }
-        const u32 hz = (h - 1) % G, hy = ((h - 1) / G) % G, hx = (h - 1) / (G * G);
+        const u32 h = G * G * hx + G * hy + hz + 1; // get_hash's cell index
         const float gx = fmaxf(fmaxf(((float)hx - M) - qx, qx - ((float)hx + (1.0f + M))), 0.0f) * grid.cx;
         const float gy = fmaxf(fmaxf(((float)hy - M) - qy, qy - ((float)hy + (1.0f + M))), 0.0f) * grid.cy;
         const float gz = fmaxf(fmaxf(((float)hz - M) - qz, qz - ((float)hz + (1.0f + M))), 0.0f) * grid.cz;

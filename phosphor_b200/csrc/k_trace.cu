@@ -827,6 +827,10 @@ void launch_shadow(const LaunchCtx &lc, const TraceOut &out, int kind, bool pres
         launch_shadow_kind<SHADOW_OPAQUE, true>(lc, out, grid, nee_blocks, one, st);
     else if (kind == SHADOW_OPAQUE)
         launch_shadow_kind<SHADOW_OPAQUE, false>(lc, out, grid, nee_blocks, one, st);
+    else if (kind == SHADOW_CLEAR && per_pixel)
+        launch_shadow_kind<SHADOW_CLEAR, true>(lc, out, grid, nee_blocks, one, st);
+    else if (kind == SHADOW_CLEAR)
+        launch_shadow_kind<SHADOW_CLEAR, false>(lc, out, grid, nee_blocks, one, st);
     else if (per_pixel)
         launch_shadow_kind<SHADOW_GENERAL, true>(lc, out, grid, nee_blocks, one, st);
     else

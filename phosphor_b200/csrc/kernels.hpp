@@ -61,7 +61,8 @@ void launch_trace(const LaunchCtx &lc, const TraceOut &out, int block, int persi
                   u32 *queue, cudaStream_t st);
 // Deferred diffuse-hit NEE: trace every recorded shadow ray (one thread per sample slot), then sum
 // each pixel's samples in sample order into hp_direct.
-// kind: SHADOW_OPAQUE when no scene has a transmissive material, else SHADOW_GENERAL.  presample:
+// kind: SHADOW_OPAQUE when no scene has a transmissive material, else SHADOW_CLEAR when no material
+// has a texture, else SHADOW_GENERAL.  presample:
 // some scene's light samples take varying RNG draws, so k_nee_sample draws its samples first.
 // per_pixel: a single scene whose only light is not an area light (one shadow ray per hit point)
 // one: the scene descriptor of a single-scene context (passed to the kernel by value), or null
