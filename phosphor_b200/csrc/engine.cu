@@ -673,8 +673,11 @@ void Engine::enq_trace_r(RoundSet &R, cudaStream_t s) {
 void Engine::enq_emit_r(RoundSet &R, cudaStream_t s) {
     ev(ST_EMIT, false, s);
     EmitOut o{R.slot_pos, R.slot_pd, R.counts};
+    bool prestart = true;
+    for (const auto &sl : sc)
+        prestart = prestart && sl.desc.max_bounces >= 3;
     launch_emit(lc(R), o, (int)tune.emit_block, (int)tune.persistent, (int)tune.emit_blocks_per_sm, R.queue + 1,
-                untextured(), s);
+                untextured(), prestart, s);
     ev(ST_EMIT, true, s);
     ev(ST_EMIT_SCAN, false, s);
     launch_scan(R.counts, R.offsets, (u64)total_emit + 1, R.scan_scr, R.ntotal, d_err.as<u32>(), s);

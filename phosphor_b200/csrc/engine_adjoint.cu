@@ -178,7 +178,7 @@ int Engine::adjoint_backward(const float *dl_dimage, float *grad, uint32_t n_gra
         enq_trace();
         // photons of the round, keeping their unquantised power
         EmitOut eo{slot_pos.as<float4>(), slot_pd.as<uint2>(), counts.as<u32>(), adj_slot_pow.as<float4>()};
-        launch_emit(lc(), eo, (int)tune.emit_block, 0, 0, nullptr, untextured(), st);
+        launch_emit(lc(), eo, (int)tune.emit_block, 0, 0, nullptr, untextured(), false, st);
         launch_scan(counts.as<u32>(), offsets.as<u32>(), (u64)total_emit + 1, scan_scr.p, d_ntotal.as<u32>(),
                     d_err.as<u32>(), st);
         launch_compact(lc(), gb(), st);

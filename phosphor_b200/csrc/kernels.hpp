@@ -79,9 +79,11 @@ struct EmitOut {
     u32 *counts;       // per photon path (global emit index)
     float4 *slot_pow;  // optional (one-thread-per-path form only): unquantised power per slot
 };
-// untextured: no material of the context has a texture
+// untextured: no material of the context has a texture.  prestart: every scene has at least three
+// photon slots per path (max_bounces >= 3), so the lane-refill form can draw the paths' light
+// samples in a pre-pass (k_emit_start) and keep them in those slots.
 void launch_emit(const LaunchCtx &lc, const EmitOut &out, int block, int persistent, int blocks_per_sm, u32 *queue,
-                 bool untextured, cudaStream_t st);
+                 bool untextured, bool prestart, cudaStream_t st);
 
 // grid build
 struct GridBufs {
