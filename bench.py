@@ -48,17 +48,17 @@ CONFIGS = {
                    desc="procedural atrium, 262,898 triangles, 1920x1080, 2^22 photons/iter, depth 16"),
 }
 METRIC = "Mphotons/s"
-# dram__bytes_read.sum + dram__bytes_write.sum of a reference stage's kernels per round, from a
-# one-launch-per-kernel ncu capture of the caustic workload at 1/2 resolution and 1/4 photons
-# (512x512 pixels, 2^18 photon paths, 425,890 stored photons), scaled by 4 to the full workload
-# (pixels for trace_rays, photon paths or stored photons for the others; the 125,001-cell scan does
-# not scale).  trace_rays = k_trace_persistent 228.3 MB + k_shadow 158.6 + k_nee_resolve 77.7 +
-# k_spec_resolve 13.6; emit_photons = k_emit_persistent 130.1 + k_scan 1.1 + k_compact 28.6;
-# scatter_photons = the two radix passes 10.6 + k_sorted_records 11.9.  The integer stages' arrays
-# stay in the 126 MB L2 between kernels, so their DRAM bytes fall below the compulsory bytes.
-# gather_flux was captured only in its optional warp-cooperative form: left out.
-NCU_TRAFFIC: dict = {"caustic": {"trace_rays": 1912.9e6, "emit_photons": 639.0e6, "hash_photons": 28.3e6,
-                                 "scan": 0.51e6, "scatter_photons": 89.9e6}}
+# dram__bytes_read.sum + dram__bytes_write.sum of a reference stage's kernels per round, from an
+# ncu capture of one whole round of the caustic workload at 1/2 resolution and 1/4 photons (512x512
+# pixels, 2^18 photon paths, ~425k stored photons), scaled by 4 to the full workload (pixels for
+# trace_rays, photon paths or stored photons for the others; the 125,001-cell scan does not scale).
+# trace_rays = k_trace_persistent 220.3 MB + k_shadow 105.9 + k_nee_resolve 76.3 + k_spec_resolve
+# 13.3; emit_photons = k_emit_persistent 103.5 + k_emit_start 0.05 + k_scan 1.1 + k_compact 29.4;
+# scatter_photons = the two radix passes 9.5 + k_sorted_records 11.9; gather_flux = k_pixel_keys 8.3
+# + the pixel radix sort 6.4 + k_gather 58.7.  The integer stages' arrays stay in the 126 MB L2
+# between kernels, so their DRAM bytes fall below the compulsory bytes.
+NCU_TRAFFIC: dict = {"caustic": {"trace_rays": 1663.3e6, "emit_photons": 536.2e6, "hash_photons": 28.2e6,
+                                 "scan": 0.51e6, "scatter_photons": 85.6e6, "gather_flux": 293.8e6}}
 
 
 def load_peaks() -> tuple[float, str]:

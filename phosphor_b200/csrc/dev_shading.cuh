@@ -523,8 +523,8 @@ PHX_SHADE_LIGHT void sample_light(Rng *rng, const SceneDesc &sc, float4 *origin,
     *power /= scale;
 }
 
-// light_sampling.h:231-300
-PHX_SHADE_NEE bool sample_light_fragment(Rng *rng, const SceneDesc &sc, float4 pos, float4 normal, LightFragment *out) {
+// light_sampling.h:231-300; always inlined (sample_light_fragment is the possibly out-of-line copy).
+PHX_DI bool light_fragment(Rng *rng, const SceneDesc &sc, float4 pos, float4 normal, LightFragment *out) {
     if (sc.n_lights == 0 || sc.total_lum < EPS)
         return false;
     float scale;
@@ -578,6 +578,9 @@ PHX_SHADE_NEE bool sample_light_fragment(Rng *rng, const SceneDesc &sc, float4 p
     out->dist = dist;
     out->n_dot_dir = ndd;
     return true;
+}
+PHX_SHADE_NEE bool sample_light_fragment(Rng *rng, const SceneDesc &sc, float4 pos, float4 normal, LightFragment *out) {
+    return light_fragment(rng, sc, pos, normal, out);
 }
 
 // light_sampling.h:302-333

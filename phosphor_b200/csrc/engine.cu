@@ -649,7 +649,8 @@ void Engine::enq_trace_r(RoundSet &R, cudaStream_t s) {
         o.def_tag = R.def_tag;
         cudaMemsetAsync(R.spec_next, 0, sizeof(u32), s);
     }
-    launch_trace(l, o, (int)tune.trace_block, (int)tune.persistent, (int)tune.trace_blocks_per_sm, R.queue, s);
+    launch_trace(l, o, (int)tune.trace_block, (int)tune.persistent, (int)tune.trace_blocks_per_sm, R.queue,
+                 untextured(), s);
     ev(ST_TRACE, true, s);
     ev(ST_SHADOW, false, s);
     bool transmissive = false, presample = false;
@@ -673,11 +674,8 @@ void Engine::enq_trace_r(RoundSet &R, cudaStream_t s) {
 void Engine::enq_emit_r(RoundSet &R, cudaStream_t s) {
     ev(ST_EMIT, false, s);
     EmitOut o{R.slot_pos, R.slot_pd, R.counts};
-    bool prestart = true;
-    for (const auto &sl : sc)
-        prestart = prestart && sl.desc.max_bounces >= 3;
     launch_emit(lc(R), o, (int)tune.emit_block, (int)tune.persistent, (int)tune.emit_blocks_per_sm, R.queue + 1,
-                untextured(), prestart, s);
+                untextured(), photon_prestart(), s);
     ev(ST_EMIT, true, s);
     ev(ST_EMIT_SCAN, false, s);
     launch_scan(R.counts, R.offsets, (u64)total_emit + 1, R.scan_scr, R.ntotal, d_err.as<u32>(), s);
@@ -836,6 +834,13 @@ bool Engine::untextured() const {
                 m.occlusion_index != PHX_NO_TEXTURE || m.metal_rough_index != PHX_NO_TEXTURE ||
                 m.transmission_index != PHX_NO_TEXTURE)
                 return false;
+    return true;
+}
+
+bool Engine::photon_prestart() const {
+    for (const auto &s : sc)
+        if (s.desc.max_bounces < 3)
+            return false;
     return true;
 }
 
@@ -1554,12 +1559,13 @@ int Engine::info(uint32_t s, phx_info *o) {
     o->bvh_build_ms = S.bvh_ms;
     // seeds, trace, [sample, shadow, resolve], emit, count scan, compaction, hash, cell scan, 3 per
     // sort pass, records, gather (+1 with the specular NEE deferred: its resolve; k_shadow traces
-    // its rays).  The sampling kernel runs only for scenes whose light samples vary in RNG draws.
+    // its rays; +1 for the photon start pre-pass of the lane-refill form).  The sampling kernel runs
+    // only for scenes whose light samples vary in RNG draws.
     bool presample = false;
     for (const auto &sl : sc)
         presample = presample || sl.desc.light_draws == LIGHT_DRAWS_VARY;
     o->kernels_per_round = 9 + 3 * o->sort_passes + (tune.nee_wavefront ? (presample ? 3 : 2) : 0) +
-                           (spec_deferred() ? 1 : 0) +
+                           (spec_deferred() ? 1 : 0) + (tune.persistent && photon_prestart() ? 1 : 0) +
                            (tune.gather_sorted && pix_key_bits ? 1 + 3 * radix_passes(pix_key_bits) : 0);
     CK(cudaStreamSynchronize(st));
     uint32_t v[3] = {0, 0, 0};

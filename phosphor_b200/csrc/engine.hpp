@@ -143,6 +143,7 @@ class Engine {
     int shard_round();
     bool any_active() const;
     bool untextured() const; // no material of any scene has a texture (indices are fixed at set-up)
+    bool photon_prestart() const; // every scene keeps >= 3 photon slots per path (k_emit_start)
 
     // differentiation (single-scene engines; engine_adjoint.cu)
     int set_materials(const phx_material *m, uint32_t n);

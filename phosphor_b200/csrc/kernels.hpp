@@ -57,8 +57,9 @@ struct TraceOut {
 };
 
 // Persistent work queue (lane refill): a device counter the kernel drains.
+// untextured: no material of the context has a texture
 void launch_trace(const LaunchCtx &lc, const TraceOut &out, int block, int persistent, int blocks_per_sm,
-                  u32 *queue, cudaStream_t st);
+                  u32 *queue, bool untextured, cudaStream_t st);
 // Deferred diffuse-hit NEE: trace every recorded shadow ray (one thread per sample slot), then sum
 // each pixel's samples in sample order into hp_direct.
 // kind: SHADOW_OPAQUE when no scene has a transmissive material, else SHADOW_CLEAR when no material
