@@ -596,9 +596,6 @@ __global__ void __launch_bounds__(128, PHX_TRACE_MINB) k_trace_persistent(Launch
 }
 
 // ---- shadow wavefront ---------------------------------------------------------------------------
-#ifndef PHX_SHADOW_INLINE_NEE
-#define PHX_SHADOW_INLINE_NEE 0
-#endif
 // One thread per recorded NEE sample; the ds samples of a pixel are consecutive threads, so a warp
 // traces shadow rays from one or two hit points toward the same light: coherent traversal.
 template <int KIND, bool PER_PIXEL, bool ONE>
@@ -647,8 +644,8 @@ __global__ void __launch_bounds__(128, PHX_SHADOW_MINB)
         rng.state = out.stash_rng[gpix];
         rng = rng_advance(rng, (g - sc.nee_base - pixel * ds) * sc.light_draws);
         LightFragment f;
-        if (PHX_SHADOW_INLINE_NEE ? light_fragment(&rng, sc, pos, out.stash_sn[gpix], &f)
-                                  : sample_light_fragment(&rng, sc, pos, out.stash_sn[gpix], &f)) { // light_sampling.h:345-352
+        // the light sampler inlined here (out of line in the camera kernels): shadow stage 6.59 -> 6.47 ms
+        if (light_fragment(&rng, sc, pos, out.stash_sn[gpix], &f)) { // light_sampling.h:345-352
             dir = f4(f.dir.x, f.dir.y, f.dir.z, 0.0f);
             dist = f.dist;
             w = f.radiance * (out.base_color[gpix] / PI);
@@ -705,7 +702,7 @@ PHX_DI void shadow_spec_slots(const LaunchCtx &lc, const TraceOut &out, u32 firs
                 rng = rng_advance(rng, (g - base) * sc.light_draws);
                 LightFragment f;
                 float4 m;
-                if (spec_light_sample<(PHX_SHADOW_INLINE_NEE != 0)>(&rng, sc, org, out.spec_org[base + 1], out.spec_org[base + 2],
+                if (spec_light_sample<true>(&rng, sc, org, out.spec_org[base + 1], out.spec_org[base + 2],
                                       out.spec_org[base + 3], hdr.y, &f, &m)) {
                     dir = f4(f.dir.x, f.dir.y, f.dir.z, 0.0f);
                     dist = f.dist;
