@@ -344,20 +344,16 @@ PHX_DI bool intersect_t(const SceneDesc &sc, float4 o, float4 d, float t_min, fl
                 const float4 mnx = __ldg(wn + px), mxx = __ldg(wn + (1 - px)), mny = __ldg(wn + py);
                 const float4 mxy = __ldg(wn + (5 - py)), mnz = __ldg(wn + pz), mxz = __ldg(wn + (9 - pz));
                 ch = __ldg(reinterpret_cast<const int4 *>(wn + 6));
-                // (mnx.. now hold the entry planes, mxx.. the exit planes.)  An empty slot (reference
-                // POP) never counts as hit, whatever its box.
-                t0 = ch.x == POP ? NOHIT
-                                 : box1(mnx.x, mxx.x, mny.x, mxy.x, mnz.x, mxz.x, ix, iy, iz, oix, oiy, oiz, t_min,
-                                        closest);
-                t1 = ch.y == POP ? NOHIT
-                                 : box1(mnx.y, mxx.y, mny.y, mxy.y, mnz.y, mxz.y, ix, iy, iz, oix, oiy, oiz, t_min,
-                                        closest);
-                t2 = ch.z == POP ? NOHIT
-                                 : box1(mnx.z, mxx.z, mny.z, mxy.z, mnz.z, mxz.z, ix, iy, iz, oix, oiy, oiz, t_min,
-                                        closest);
-                t3 = ch.w == POP ? NOHIT
-                                 : box1(mnx.w, mxx.w, mny.w, mxy.w, mnz.w, mxz.w, ix, iy, iz, oix, oiy, oiz, t_min,
-                                        closest);
+                // (mnx.. now hold the entry planes, mxx.. the exit planes.)
+                // Empty slots carry the box (1e30, -1e30), which no ray with a finite inverse
+                // direction component enters (a NaN slab is ignored, and not all three can be NaN);
+                // their reference is still checked where a child is stacked, and descending into it
+                // pops the next entry, so it is never used as a node index.  Testing the reference
+                // here instead measured 4 % slower in the shadow and photon kernels.
+                t0 = box1(mnx.x, mxx.x, mny.x, mxy.x, mnz.x, mxz.x, ix, iy, iz, oix, oiy, oiz, t_min, closest);
+                t1 = box1(mnx.y, mxx.y, mny.y, mxy.y, mnz.y, mxz.y, ix, iy, iz, oix, oiy, oiz, t_min, closest);
+                t2 = box1(mnx.z, mxx.z, mny.z, mxy.z, mnz.z, mxz.z, ix, iy, iz, oix, oiy, oiz, t_min, closest);
+                t3 = box1(mnx.w, mxx.w, mny.w, mxy.w, mnz.w, mxz.w, ix, iy, iz, oix, oiy, oiz, t_min, closest);
             }
             i32 r0 = ch.x, r1 = ch.y, r2 = ch.z, r3 = ch.w;
             if constexpr (!ORDERED) {
@@ -368,7 +364,7 @@ PHX_DI bool intersect_t(const SceneDesc &sc, float4 o, float4 d, float t_min, fl
                 float tn = NOHIT;
 #pragma unroll
                 for (int c = 3; c >= 0; c--) {
-                    if (ts[c] == NOHIT)
+                    if (ts[c] == NOHIT || rs[c] == POP)
                         continue;
                     if (nxt != POP) {
                         if (sp < TRAV_STACK) {
@@ -384,6 +380,31 @@ PHX_DI bool intersect_t(const SceneDesc &sc, float4 o, float4 d, float t_min, fl
                 }
                 node = nxt;
             } else {
+            if constexpr (LISTED) {
+                // the nearest hit child first; the others stacked in slot order (a shadow ray's list
+                // rarely fills, so the full sort of the others rarely culls anything: shadow stage
+                // 6.22 -> 6.09 ms on the caustic workload)
+                float tm = t0;
+                i32 rm = r0;
+                if (t1 < tm) { tm = t1; rm = r1; }
+                if (t2 < tm) { tm = t2; rm = r2; }
+                if (t3 < tm) { tm = t3; rm = r3; }
+                const float ts[4] = {t3, t2, t1, t0};
+                const i32 rs[4] = {r3, r2, r1, r0};
+                node = tm == NOHIT ? POP : rm;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    if (ts[k] == NOHIT || rs[k] == POP || rs[k] == rm)
+                        continue;
+                    if (sp < TRAV_STACK) {
+                        stack_ref[sp] = rs[k];
+                        stack_t[sp] = ts[k];
+                        sp++;
+                    } else {
+                        *overflow += 1;
+                    }
+                }
+            } else {
             sort2(t0, r0, t1, r1); // sorting network: ascending entry distance, misses (+inf) last
             sort2(t2, r2, t3, r3);
             sort2(t0, r0, t2, r2);
@@ -398,7 +419,7 @@ PHX_DI bool intersect_t(const SceneDesc &sc, float4 o, float4 d, float t_min, fl
                 const i32 rs[3] = {r3, r2, r1};
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
-                    if (ts[k] == NOHIT)
+                    if (ts[k] == NOHIT || rs[k] == POP)
                         continue;
                     if (sp < TRAV_STACK) {
                         stack_ref[sp] = rs[k];
@@ -408,6 +429,7 @@ PHX_DI bool intersect_t(const SceneDesc &sc, float4 o, float4 d, float t_min, fl
                         *overflow += 1;
                     }
                 }
+            }
             }
             }
         } else if (node >= 0) { // child pair: test both children, descend into the nearer hit one
