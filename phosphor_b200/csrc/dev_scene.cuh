@@ -225,17 +225,6 @@ PHX_DI float slab_inv(float dc, float oc) {
     return (fabsf(r) == __int_as_float(0x7f800000) && fabsf(oc) < 1e4f) ? copysignf(1e30f, r) : r;
 }
 
-PHX_DI void sort2(float &ta, i32 &ra, float &tb, i32 &rb) {
-    if (tb < ta) {
-        float t = ta;
-        ta = tb;
-        tb = t;
-        i32 r = ra;
-        ra = rb;
-        rb = r;
-    }
-}
-
 // The hits of a ray on [t_min, t_max] that one traversal collects for a shadow ray crossing
 // transmissive surfaces: the K first in the order of (t ascending, reference leaf rank descending)
 // — the order in which closest-hit queries with a rising t_min return them.  Every hit with
@@ -292,9 +281,10 @@ PHX_DI void hit_list_insert(const SceneDesc &sc, HitList<K> &L, float t, i32 tri
 // each iteration advancing every unfinished lane by exactly one node (an inner child pair or a
 // leaf), so neighbouring rays share every node fetch and the warp never runs one lane's inner
 // loop while the others wait.
-// ORDERED: a 4-wide node's hit children are visited nearest first (sorting network); otherwise in
-// slot order.  The result never depends on the order (closest hit and tie rank, the hit list, or
-// for `any` whether there is a hit); the order only decides how early far subtrees are culled.
+// ORDERED: a 4-wide node's nearest hit child is visited first (the others in slot order);
+// otherwise all in slot order.  The result never depends on the order (closest hit and tie rank,
+// the hit list, or for `any` whether there is a hit); the order only decides how early far
+// subtrees are culled.
 template <class LIST, bool ORDERED = true>
 PHX_DI bool intersect_t(const SceneDesc &sc, float4 o, float4 d, float t_min, float t_max, Hit *hit, u32 *overflow,
                         bool any, LIST *list) {
@@ -380,10 +370,9 @@ PHX_DI bool intersect_t(const SceneDesc &sc, float4 o, float4 d, float t_min, fl
                 }
                 node = nxt;
             } else {
-            if constexpr (LISTED) {
-                // the nearest hit child first; the others stacked in slot order (a shadow ray's list
-                // rarely fills, so the full sort of the others rarely culls anything: shadow stage
-                // 6.22 -> 6.09 ms on the caustic workload)
+                // the nearest hit child first; the others stacked in slot order.  A full sort of the
+                // four (stacked farthest first) culled little more and cost more instructions: shadow
+                // stage 6.22 -> 6.09 ms, photon kernel 3.86 -> 3.74 ms on the caustic workload.
                 float tm = t0;
                 i32 rm = r0;
                 if (t1 < tm) { tm = t1; rm = r1; }
@@ -404,33 +393,6 @@ PHX_DI bool intersect_t(const SceneDesc &sc, float4 o, float4 d, float t_min, fl
                         *overflow += 1;
                     }
                 }
-            } else {
-            sort2(t0, r0, t1, r1); // sorting network: ascending entry distance, misses (+inf) last
-            sort2(t2, r2, t3, r3);
-            sort2(t0, r0, t2, r2);
-            sort2(t1, r1, t3, r3);
-            sort2(t1, r1, t2, r2);
-            if (t0 == NOHIT) {
-                node = POP;
-            } else {
-                node = r0;
-                // the others, farthest first, so the nearest of them is popped first
-                const float ts[3] = {t3, t2, t1};
-                const i32 rs[3] = {r3, r2, r1};
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    if (ts[k] == NOHIT || rs[k] == POP)
-                        continue;
-                    if (sp < TRAV_STACK) {
-                        stack_ref[sp] = rs[k];
-                        stack_t[sp] = ts[k];
-                        sp++;
-                    } else {
-                        *overflow += 1;
-                    }
-                }
-            }
-            }
             }
         } else if (node >= 0) { // child pair: test both children, descend into the nearer hit one
             const float4 *cn = sc.cnodes + 4 * (size_t)node;
