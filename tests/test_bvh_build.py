@@ -289,3 +289,48 @@ def test_device_tree_in_a_batch():
         b.close()
     for a, d in zip(out[A.PHX_F_HOST_BVH], out[0]):
         assert np.array_equal(a.view(np.uint32), d.view(np.uint32))
+
+
+def _slab_inv(d, o):
+    """The kernels' inverse direction component: 1/d, with +-1e30 for a zero component while |o| < 1e4."""
+    with np.errstate(divide="ignore"):
+        r = np.float32(1.0) / d
+    return np.where(np.isinf(r) & (np.abs(o) < 1e4), np.copysign(np.float32(1e30), r), r).astype(np.float32)
+
+
+@pytest.mark.parametrize("scene_fn", [lambda: random_soup(3000, 2), lambda: grid_soup(24),
+                                      lambda: P.SceneData.generate(A.PHX_SCENE_CAUSTIC, 1, 64, 64, detail=16)])
+def test_empty_slots_are_never_entered(scene_fn):
+    """The 4-wide traversal skips the reference check of an empty child slot in its slab test and
+    checks the reference only where a child is stacked or entered.  That relies on every empty slot
+    carrying the box (1e30, -1e30), which the sign-selected slab test (float32, fused multiply-add,
+    NaN slabs ignored) never enters: checked for random, axis-aligned and far-away rays."""
+    b = R.traversal_bvh(scene_fn(), 4, True, -1)
+    nodes = b.nodes.reshape(-1, 7, 4)
+    refs = nodes[:, 6, :].view(np.int32)
+    empty = refs == EMPTY
+    assert empty.any(), "the tree has no empty slot to check"
+    lo, hi = nodes[:, 0:6:2, :], nodes[:, 1:6:2, :]  # rows minx, miny, minz / maxx, maxy, maxz
+    assert np.all(lo[np.broadcast_to(empty[:, None, :], lo.shape)] == np.float32(1e30))
+    assert np.all(hi[np.broadcast_to(empty[:, None, :], hi.shape)] == np.float32(-1e30))
+    rng = np.random.default_rng(5)
+    n = 20000
+    for scale in (1.0, 1e3, 1e4, 1e5, 1e20):
+        o = (rng.uniform(-1, 1, (n, 3)) * scale).astype(np.float32)
+        d = rng.uniform(-1, 1, (n, 3)).astype(np.float32)
+        d[0::5, 0] = 0.0
+        d[1::5, :2] = 0.0
+        d[2::5, 2] = -0.0
+        d /= np.linalg.norm(d, axis=1, keepdims=True).astype(np.float32)
+        inv = _slab_inv(d, o)
+        oi = (o * inv).astype(np.float32)
+        with np.errstate(invalid="ignore", over="ignore"):
+            # an empty slot's entry plane is 1e30 for a positive inverse component and -1e30 for a
+            # negative one, its exit plane the other; distances plane * inv - o * inv in float32
+            near = np.where(inv >= 0, np.float32(1e30), np.float32(-1e30)).astype(np.float32)
+            far = np.where(inv >= 0, np.float32(-1e30), np.float32(1e30)).astype(np.float32)
+            tn = (near.astype(np.float64) * inv - oi).astype(np.float32)  # fma rounding: one rounding
+            tf = (far.astype(np.float64) * inv - oi).astype(np.float32)
+        tn = np.fmax(np.fmax(np.fmax(tn[:, 0], tn[:, 1]), tn[:, 2]), np.float32(1e-5))
+        tf = np.fmin(np.fmin(np.fmin(tf[:, 0], tf[:, 1]), tf[:, 2]), np.float32(np.inf))
+        assert not np.any(tn <= tf), f"an empty slot's box is entered (origin scale {scale})"
